@@ -1,0 +1,136 @@
+/* Generated from gegs_b200/physics_layout.py -- edit the field list there.
+ *
+ * Physics-table block read by the transport kernels.  Same content and
+ * index conventions as the reference's __device__ globals
+ * (commonBlocks dev.h:11-262, media.cu:96-100); float2 pairs are float[2].
+ * Every member is 4 bytes wide, so the struct has no padding. */
+#ifndef GEGS_PHYSICS_H
+#define GEGS_PHYSICS_H
+
+#include <stdint.h>
+
+#define GEGS_MXMED 6
+#define GEGS_MXGE 200
+#define GEGS_MXEKE 150
+#define GEGS_MXEL 10
+#define GEGS_MXRAYFF 100
+#define GEGS_RAYCDFSIZE 100
+#define GEGS_MXELEMENT 100
+#define GEGS_MXSHELL 6
+#define GEGS_MXTRANS 39
+#define GEGS_MXEDGE 16
+#define GEGS_MXTOTSH 1538
+#define GEGS_MXMDSH 50
+#define GEGS_MAX_EII_SHELLS 40
+#define GEGS_N_EII_BINS 250
+#define GEGS_MAXL_MS 63
+#define GEGS_MAXQ_MS 7
+#define GEGS_MAXU_MS 31
+#define GEGS_MS_SIZE 16384
+#define GEGS_MAX_EII_BINS 10000
+
+typedef struct gegs_physics {
+    int32_t nmed;
+    float rm;
+    float prm;
+    float rmt2;
+    float rmsq;
+    float estepe;
+    float ximax;
+    float skindepth_for_bca;
+    int32_t transport_algorithm;
+    int32_t exact_bca;
+    int32_t spin_effects;
+    int32_t ibrdst;
+    int32_t iprdst;
+    int32_t nbr_split;
+    int32_t eii_flag;
+    float rho[6];
+    float ae[6];
+    float ap[6];
+    float ue[6];
+    float up[6];
+    float te[6];
+    float thmoll[6];
+    float rlc[6];
+    float delcm[6];
+    float zbrang[6];
+    float lzbrang[6];
+    float log_ap[6];
+    float blcc[6];
+    float xcc[6];
+    float expeke1[6];
+    float smaxir[6];
+    float e_max_rr[6];
+    int32_t i_do_rr[6];
+    int32_t nne[6];
+    float zelem[60];
+    float pz[60];
+    float wa[60];
+    float dl1[48];
+    float dl2[48];
+    float dl3[48];
+    float dl4[48];
+    float dl5[48];
+    float dl6[48];
+    float bpar[12];
+    float ge[6][2];
+    float gmfp[1200][2];
+    float gbr1[1200][2];
+    float gbr2[1200][2];
+    float cohe[1200][2];
+    float pmax[1200][2];
+    float rayleigh_data[600][4];
+    int32_t i_array[600];
+    float eke01[6][2];
+    float sig[1800][2];
+    float dedx[1800][2];
+    float ebr1[900][2];
+    float pbr1[900][2];
+    float pbr2[900][2];
+    float tmxs[900][2];
+    float range_ep[1800];
+    float e_array[900];
+    float sig_e[12];
+    int32_t sig_ismonotone[12];
+    float binding_energies[600];
+    float interaction_prob[600];
+    float relaxation_prob[3900];
+    float edge_energies[1600];
+    float edge_a[1600];
+    float edge_b[1600];
+    float edge_c[1600];
+    float edge_d[1600];
+    int32_t edge_number[100];
+    int32_t iz_array[1538];
+    int32_t shn_array[1538];
+    int32_t ne_array[1538];
+    float be_array[1538];
+    float jo_array[1538];
+    float erfjo_array[1538];
+    int32_t shell_array[300];
+    float eno_array[300];
+    int32_t eno_atbin_array[300];
+    int32_t n_shell[6];
+    float llammin;
+    float llammax;
+    float dllamb;
+    float dllambi;
+    float dqms;
+    float dqmsi;
+    float ums_array[16384];
+    float fms_array[16384];
+    float wms_array[16384];
+    int32_t ims_array[16384];
+    float eii_xsection[10000][2];
+    float eii_cons[6];
+    float eii[40][2];
+    int32_t eii_z[40];
+    int32_t eii_sh[40];
+    int32_t eii_nshells[100];
+    int32_t eii_nsh[6];
+    int32_t eii_first[60];
+    int32_t eii_no[60];
+} gegs_physics;
+
+#endif /* GEGS_PHYSICS_H */
