@@ -78,7 +78,7 @@ class Medium:
 MEDIA = {
     "AIR700ICRU": Medium("AIR700ICRU", 0.00120479, {6: 0.000124, 7: 0.755268, 8: 0.231781, 18: 0.012827}, gas=True),
     "H2O700ICRU": Medium("H2O700ICRU", 1.0, {1: 0.111894, 8: 0.888106}),
-    "LUNG700ICRU": Medium("LUNG700ICRU", 0.26, {1: 0.103, 6: 0.105, 7: 0.031, 8: 0.761}),
+    "LUNG700ICRU": Medium("LUNG700ICRU", 1.05, {1: 0.103, 6: 0.105, 7: 0.031, 8: 0.761}),
     "ICRUTISSUE700ICRU": Medium("ICRUTISSUE700ICRU", 1.0, {1: 0.101, 6: 0.111, 7: 0.026, 8: 0.762}),
     "ICRPBONE700ICRU": Medium("ICRPBONE700ICRU", 1.85, {1: 0.047234, 6: 0.14433, 7: 0.04199, 8: 0.446096,
                                                         15: 0.10497, 20: 0.20993}),

@@ -1,0 +1,30 @@
+/* C entry points of the CPU oracle (test infrastructure only; see ora_internal.h). */
+#ifndef GEGS_ORACLE_H
+#define GEGS_ORACLE_H
+
+#include <stdint.h>
+#include <stddef.h>
+#include "../include/gegs_physics.h"
+#include "../include/gegs_scene.h"
+
+typedef struct ora_stats {
+    uint64_t counts[10];          /* particles processed per stage (photon .. annih) */
+    uint64_t steps_photon, steps_electron;
+    double e_escaped;             /* energy scored to regions 0..5 (not tallied) */
+    int32_t error;
+    int32_t pad_;
+} ora_stats;
+
+size_t ora_sizeof_physics(void);
+size_t ora_sizeof_scene(void);
+size_t ora_sizeof_field(void);
+float ora_log(float x);
+float ora_exp(float x);
+void ora_sincos_turns(float t, float *s, float *c);
+uint32_t ora_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, int lane);
+
+/* Run histories [h0, h1); adds the int64 energy tally (MeV * 2^30) into `tally`. */
+int ora_run(const gegs_physics *P, const gegs_scene *S, uint64_t h0, uint64_t h1, int nthreads,
+            int64_t *tally, ora_stats *stats);
+
+#endif

@@ -1,0 +1,68 @@
+"""ctypes loader for the CPU oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke`` and bench.py's CPU-baseline leg import
+this module, as the checker.  ``build()`` compiles ``oracle/*.c`` with the
+committed Makefile into ``oracle/_build/libgegs_oracle.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB = HERE / "_build" / "libgegs_oracle.so"
+
+
+class Stats(C.Structure):
+    _fields_ = [("counts", C.c_uint64 * 10), ("steps_photon", C.c_uint64), ("steps_electron", C.c_uint64),
+                ("e_escaped", C.c_double), ("error", C.c_int32), ("pad_", C.c_int32)]
+
+
+def build(force=False):
+    srcs = list(HERE.glob("*.c")) + list(HERE.glob("*.h"))
+    if force or not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        L.ora_log.restype = C.c_float
+        L.ora_log.argtypes = [C.c_float]
+        L.ora_exp.restype = C.c_float
+        L.ora_exp.argtypes = [C.c_float]
+        L.ora_sincos_turns.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.ora_philox.restype = C.c_uint32
+        L.ora_philox.argtypes = [C.c_uint32] * 6 + [C.c_int]
+        L.ora_sizeof_physics.restype = C.c_size_t
+        L.ora_sizeof_scene.restype = C.c_size_t
+        L.ora_sizeof_field.restype = C.c_size_t
+        L.ora_run.restype = C.c_int
+        L.ora_run.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_int,
+                              C.POINTER(C.c_int64), C.POINTER(Stats)]
+        _lib = L
+    return _lib
+
+
+def run(physics: np.ndarray, scene_holder, h0: int, h1: int, threads: int = 0):
+    """Run histories [h0, h1) on the CPU; returns (int64 tally, stats dict)."""
+    L = lib()
+    tally = np.zeros(scene_holder.nvox, np.int64)
+    st = Stats()
+    phys = np.ascontiguousarray(physics)
+    rc = L.ora_run(phys.ctypes.data, C.addressof(scene_holder.scene), h0, h1, threads or os.cpu_count(),
+                   tally.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(st))
+    stats = dict(counts=list(st.counts), steps_photon=st.steps_photon, steps_electron=st.steps_electron,
+                 e_escaped=st.e_escaped, error=st.error, rc=rc)
+    return tally, stats
