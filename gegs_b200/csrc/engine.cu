@@ -1,0 +1,473 @@
+// Host engine behind the C ABI (include/gegs.h): device buffers, the event
+// queues, the persistent CUDA-graph wave loop and the plain host-driven loop.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "kernels.cuh"
+#include "../../include/gegs.h"
+
+namespace {
+
+// queue capacity per history in flight, per stage
+const float kCapFactor[GX_NSTAGE] = {6.f, 3.f, 3.f, 3.f, 3.f, 6.f, 3.f, 3.f, 3.f, 3.f};
+
+}  // namespace
+
+struct gegs_engine {
+    int device = 0;
+    int nsm = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+
+    gegs_physics *d_P = nullptr;
+    Vox *d_reg = nullptr;
+    float *d_xb = nullptr, *d_yb = nullptr, *d_zb = nullptr;
+    gegs_field *d_fields = nullptr;
+    float2 *d_cross = nullptr;
+    gegs_phsp_record *d_phsp = nullptr;
+    uint64_t nphsp = 0, phsp_cap = 0;
+    unsigned long long *d_tally = nullptr;
+    uint64_t nvox = 0;
+    uint32_t *d_err = nullptr;
+    unsigned long long *d_stats = nullptr;
+    SchedState *d_sched = nullptr;
+    TraceRec *d_trace = nullptr;
+    uint32_t *d_trace_n = nullptr;
+    uint32_t trace_cap = 0;
+    uint32_t *d_qmeta = nullptr;       // count[10], head[10], done[10]
+    Part *d_qbuf[GX_NSTAGE] = {};
+    uint32_t qcap[GX_NSTAGE] = {};
+    uint32_t batch = 0;
+
+    DevCtx ctx{};
+    bool have_physics = false, have_scene = false;
+    unsigned long long ctx_gen = 1;
+
+    // cached persistent graph
+    cudaGraphExec_t gexec = nullptr;
+    unsigned long long graph_gen = 0;
+    int graph_grid = 0, graph_threads = 0;
+
+    gegs_run_stats last{};
+};
+
+static gegs_status cuda_fail(gegs_engine *e, cudaError_t c, const char *what)
+{
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(c));
+    e->err = buf;
+    return c == cudaErrorMemoryAllocation ? GEGS_ERR_NOMEM : GEGS_ERR_CUDA;
+}
+
+#define CK(call, what)                                        \
+    do {                                                      \
+        cudaError_t _c = (call);                              \
+        if (_c != cudaSuccess) return cuda_fail(e, _c, what); \
+    } while (0)
+
+template <typename T>
+static cudaError_t realloc_dev(T **p, size_t n)
+{
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    if (n == 0) return cudaSuccess;
+    return cudaMalloc((void **)p, n * sizeof(T));
+}
+
+extern "C" {
+
+const char *gegs_version(void) { return "gegs_b200 0.1 (sm_100a)"; }
+size_t gegs_sizeof_physics(void) { return sizeof(gegs_physics); }
+size_t gegs_sizeof_scene(void) { return sizeof(gegs_scene); }
+size_t gegs_sizeof_field(void) { return sizeof(gegs_field); }
+
+const char *gegs_last_error(const gegs_engine *e) { return e ? e->err.c_str() : "null engine"; }
+
+gegs_status gegs_create(int device, gegs_engine **out)
+{
+    if (!out) return GEGS_ERR_ARG;
+    *out = nullptr;
+    gegs_engine *e = new gegs_engine();
+    e->device = device;
+    cudaError_t c = cudaSetDevice(device);
+    if (c != cudaSuccess) { gegs_status s = cuda_fail(e, c, "cudaSetDevice"); *out = e; return s; }
+    cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, device);
+    CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "stream");
+    CK(cudaEventCreate(&e->ev0), "event");
+    CK(cudaEventCreate(&e->ev1), "event");
+    CK(cudaMalloc(&e->d_err, sizeof(uint32_t)), "err");
+    CK(cudaMalloc(&e->d_stats, sizeof(unsigned long long) * 16), "stats");
+    CK(cudaMalloc(&e->d_sched, sizeof(SchedState)), "sched");
+    CK(cudaMalloc(&e->d_qmeta, sizeof(uint32_t) * 3 * GX_NSTAGE), "qmeta");
+    CK(cudaMemset(e->d_qmeta, 0, sizeof(uint32_t) * 3 * GX_NSTAGE), "qmeta");
+    *out = e;
+    return GEGS_OK;
+}
+
+void gegs_destroy(gegs_engine *e)
+{
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    cudaFree(e->d_P); cudaFree(e->d_reg); cudaFree(e->d_xb); cudaFree(e->d_yb); cudaFree(e->d_zb);
+    cudaFree(e->d_fields); cudaFree(e->d_cross); cudaFree(e->d_phsp); cudaFree(e->d_tally);
+    cudaFree(e->d_err); cudaFree(e->d_stats); cudaFree(e->d_sched); cudaFree(e->d_qmeta);
+    cudaFree(e->d_trace); cudaFree(e->d_trace_n);
+    for (int q = 0; q < GX_NSTAGE; q++) cudaFree(e->d_qbuf[q]);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+}
+
+gegs_status gegs_set_physics(gegs_engine *e, const gegs_physics *P)
+{
+    if (!e || !P) return GEGS_ERR_ARG;
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    if (!e->d_P) CK(cudaMalloc(&e->d_P, sizeof(gegs_physics)), "physics");
+    CK(cudaMemcpyAsync(e->d_P, P, sizeof(gegs_physics), cudaMemcpyHostToDevice, e->stream), "physics H2D");
+    CK(cudaStreamSynchronize(e->stream), "physics sync");
+    e->have_physics = true;
+    e->ctx.P = e->d_P;
+    e->ctx_gen++;
+    return GEGS_OK;
+}
+
+gegs_status gegs_set_phsp(gegs_engine *e, const gegs_phsp_record *recs, uint64_t n)
+{
+    if (!e || !recs || n == 0) return GEGS_ERR_ARG;
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    if (n > e->phsp_cap) {
+        CK(realloc_dev(&e->d_phsp, n), "phsp");
+        e->phsp_cap = n;
+        e->ctx_gen++;
+    }
+    CK(cudaMemcpyAsync(e->d_phsp, recs, n * sizeof(gegs_phsp_record), cudaMemcpyHostToDevice, e->stream), "phsp H2D");
+    if (e->nphsp != n) e->ctx_gen++;
+    e->nphsp = n;
+    e->ctx.phsp = e->d_phsp;
+    e->ctx.nphsp = n;
+    return GEGS_OK;
+}
+
+gegs_status gegs_set_scene(gegs_engine *e, const gegs_scene *S)
+{
+    if (!e || !S || !e->have_physics) return GEGS_ERR_ARG;
+    if (S->nx <= 0 || S->ny <= 0 || S->nz <= 0 || S->nfields < 1 || S->nfields > GEGS_MAX_FIELDS || !S->phsp || S->nphsp == 0)
+        return GEGS_ERR_ARG;
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    gegs_physics Ph;
+    CK(cudaMemcpy(&Ph, e->d_P, sizeof Ph, cudaMemcpyDeviceToHost), "physics D2H");
+    uint64_t nvox = (uint64_t)S->nx * S->ny * S->nz;
+    std::vector<Vox> reg(nvox + GX_VAC_AND_OTH);
+    reg[0].med = GX_VACUUM; reg[0].flags = 0; reg[0].rhof = 0.0f;
+    for (int i = 1; i < GX_VAC_AND_OTH; i++) {
+        int med = S->other_med[i - 1];
+        if (med < 0) med = S->other_med[0];
+        if (med < 0 || med >= Ph.nmed) { e->err = "other_med outside the media list"; return GEGS_ERR_ARG; }
+        reg[i].med = (uint16_t)med; reg[i].flags = (uint16_t)S->region_flags; reg[i].rhof = 1.0f;
+    }
+    for (uint64_t v = 0; v < nvox; v++) {
+        Vox &r = reg[v + GX_VAC_AND_OTH];
+        uint16_t med = S->voxel_med[v];
+        r.med = med;
+        if (med == GX_VACUUM) { r.flags = 0; r.rhof = 0.0f; continue; }
+        if (med >= Ph.nmed) { e->err = "voxel medium outside the media list"; return GEGS_ERR_ARG; }
+        r.flags = (uint16_t)S->region_flags;
+        r.rhof = S->voxel_rhof[v];
+    }
+    CK(realloc_dev(&e->d_reg, reg.size()), "regions");
+    CK(cudaMemcpy(e->d_reg, reg.data(), reg.size() * sizeof(Vox), cudaMemcpyHostToDevice), "regions H2D");
+    CK(realloc_dev(&e->d_xb, (size_t)S->nx + 1), "bounds");
+    CK(realloc_dev(&e->d_yb, (size_t)S->ny + 1), "bounds");
+    CK(realloc_dev(&e->d_zb, (size_t)S->nz + 1), "bounds");
+    CK(cudaMemcpy(e->d_xb, S->x_bounds, ((size_t)S->nx + 1) * 4, cudaMemcpyHostToDevice), "bounds H2D");
+    CK(cudaMemcpy(e->d_yb, S->y_bounds, ((size_t)S->ny + 1) * 4, cudaMemcpyHostToDevice), "bounds H2D");
+    CK(cudaMemcpy(e->d_zb, S->z_bounds, ((size_t)S->nz + 1) * 4, cudaMemcpyHostToDevice), "bounds H2D");
+    CK(realloc_dev(&e->d_fields, (size_t)S->nfields), "fields");
+    CK(cudaMemcpy(e->d_fields, S->fields, sizeof(gegs_field) * S->nfields, cudaMemcpyHostToDevice), "fields H2D");
+    if (!e->d_cross) CK(cudaMalloc(&e->d_cross, sizeof(float2) * 960), "crossXZ");
+    CK(cudaMemcpy(e->d_cross, S->crossXZ, sizeof(float2) * 960, cudaMemcpyHostToDevice), "crossXZ H2D");
+    if (nvox != e->nvox || !e->d_tally) {
+        CK(realloc_dev(&e->d_tally, nvox), "tally");
+        e->nvox = nvox;
+    }
+    CK(cudaMemset(e->d_tally, 0, nvox * sizeof(unsigned long long)), "tally reset");
+    gegs_status st = gegs_set_phsp(e, S->phsp, S->nphsp);
+    if (st != GEGS_OK) return st;
+    CK(cudaStreamSynchronize(e->stream), "scene sync");
+
+    DevCtx &C = e->ctx;
+    C.P = e->d_P;
+    C.reg = e->d_reg;
+    C.xb = e->d_xb; C.yb = e->d_yb; C.zb = e->d_zb;
+    C.fields = e->d_fields;
+    C.crossXZ = e->d_cross;
+    C.phsp = e->d_phsp;
+    C.nphsp = e->nphsp;
+    C.tally = e->d_tally;
+    C.err = e->d_err;
+    C.stats = e->d_stats;
+    C.nx = S->nx; C.ny = S->ny; C.nz = S->nz; C.nfields = S->nfields;
+    C.change_xyz = S->change_xyz;
+    C.hownear_off = S->hownear_region_offset == 6 ? 6 : 5;
+    C.sid = S->source_to_isocenter;
+    C.iso0 = S->iso[0]; C.iso1 = S->iso[1]; C.iso2 = S->iso[2];
+    C.z_phsp = S->z_phsp;
+    C.mlc_rmax = S->mlc_rmax; C.mlc_zmin = S->mlc_zmin; C.mlc_zthick = S->mlc_zthick;
+    C.mlc_x_start = S->mlc_x_start; C.mlc_x_end = S->mlc_x_end; C.mlc_x_mid_1 = S->mlc_x_mid_1;
+    C.mlc_x_mid_2 = S->mlc_x_mid_2; C.mlc_air_gap = S->mlc_air_gap; C.mlc_wl_full = S->mlc_wl_full;
+    C.mlc_wl_target = S->mlc_wl_target; C.mlc_wl_isocenter = S->mlc_wl_isocenter; C.mlc_wt = S->mlc_wt;
+    for (int i = 0; i < 4; i++) {
+        C.boundaryXZ[i] = make_float2(S->boundaryXZ[i][0], S->boundaryXZ[i][1]);
+        C.boundaryYZ[i] = make_float2(S->boundaryYZ[i][0], S->boundaryYZ[i][1]);
+    }
+    for (int i = 0; i < 8; i++) C.module_order[i] = S->module_order[i];
+    C.seed_lo = (uint32_t)S->seed;
+    C.seed_hi = (uint32_t)(S->seed >> 32);
+    e->have_scene = true;
+    e->ctx_gen++;
+    return GEGS_OK;
+}
+
+gegs_status gegs_reset_tally(gegs_engine *e)
+{
+    if (!e || !e->d_tally) return GEGS_ERR_ARG;
+    CK(cudaMemsetAsync(e->d_tally, 0, e->nvox * sizeof(unsigned long long), e->stream), "tally reset");
+    CK(cudaStreamSynchronize(e->stream), "tally reset sync");
+    return GEGS_OK;
+}
+
+}  // extern "C"
+
+static gegs_status ensure_queues(gegs_engine *e, uint32_t batch)
+{
+    if (batch == e->batch) return GEGS_OK;
+    for (int q = 0; q < GX_NSTAGE; q++) {
+        uint64_t cap = (uint64_t)(kCapFactor[q] * (float)batch) + 4096;
+        if (cap > 0xFFFFFFF0ull) cap = 0xFFFFFFF0ull;
+        CK(realloc_dev(&e->d_qbuf[q], (size_t)cap), "queue buffer");
+        e->qcap[q] = (uint32_t)cap;
+    }
+    e->batch = batch;
+    e->ctx_gen++;
+    return GEGS_OK;
+}
+
+static void fill_queue_ctx(gegs_engine *e)
+{
+    QueueSet &Q = e->ctx.q;
+    for (int q = 0; q < GX_NSTAGE; q++) { Q.buf[q] = e->d_qbuf[q]; Q.cap[q] = e->qcap[q]; }
+    Q.count = e->d_qmeta;
+    Q.head = e->d_qmeta + GX_NSTAGE;
+    Q.done = e->d_qmeta + 2 * GX_NSTAGE;
+}
+
+static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
+{
+    const DevCtx &C = e->ctx;
+    cudaStream_t s = e->stream;
+    k_source<<<grid, threads, 0, s>>>(C, e->d_sched);
+    k_photon<<<grid, threads, 0, s>>>(C);
+    k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(C);
+    k_interact<ST_PHOTO><<<grid, threads, 0, s>>>(C);
+    k_interact<ST_RAYLEIGH><<<grid, threads, 0, s>>>(C);
+    k_interact<ST_PAIR><<<grid, threads, 0, s>>>(C);
+    k_electron<<<grid, threads, 0, s>>>(C);
+    k_interact<ST_MOLLER><<<grid, threads, 0, s>>>(C);
+    k_interact<ST_BREMS><<<grid, threads, 0, s>>>(C);
+    k_interact<ST_BHABHA><<<grid, threads, 0, s>>>(C);
+    k_interact<ST_ANNIH><<<grid, threads, 0, s>>>(C);
+}
+
+static gegs_status build_graph(gegs_engine *e, int grid, int threads)
+{
+    if (e->gexec && e->graph_gen == e->ctx_gen && e->graph_grid == grid && e->graph_threads == threads) return GEGS_OK;
+    if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0), "graph create");
+    cudaGraphConditionalHandle handle;
+    CK(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault), "conditional handle");
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CK(cudaGraphAddNode(&cnode, g, nullptr, 0, &cp), "conditional node");
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(e->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal), "capture");
+    launch_wave_kernels(e, grid, threads);
+    k_plan_cond<<<1, 1, 0, e->stream>>>(e->ctx, e->d_sched, handle);
+    cudaGraph_t captured;
+    CK(cudaStreamEndCapture(e->stream, &captured), "end capture");
+    CK(cudaGraphInstantiate(&e->gexec, g, 0), "graph instantiate");
+    cudaGraphDestroy(g);
+    e->graph_gen = e->ctx_gen;
+    e->graph_grid = grid;
+    e->graph_threads = threads;
+    return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts)
+{
+    if (!e || !e->have_scene || hist_end < hist_begin) return GEGS_ERR_ARG;
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    gegs_run_opts o = {};
+    if (opts) o = *opts;
+    uint32_t batch = o.batch ? o.batch : (1u << 18);
+    int threads = o.threads_per_block ? o.threads_per_block : 256;
+    int bps = o.blocks_per_sm ? o.blocks_per_sm : 4;
+    int grid = e->nsm * bps;
+    uint32_t max_waves = o.max_waves ? o.max_waves : 200000u;
+    gegs_status st = ensure_queues(e, batch);
+    if (st != GEGS_OK) return st;
+    fill_queue_ctx(e);
+
+    SchedState hs = {};
+    hs.next = hist_begin;
+    hs.end = hist_end;
+    hs.batch = batch;
+    hs.max_waves = max_waves;
+    CK(cudaMemcpyAsync(e->d_sched, &hs, sizeof hs, cudaMemcpyHostToDevice, e->stream), "sched H2D");
+    CK(cudaMemsetAsync(e->d_qmeta, 0, sizeof(uint32_t) * 3 * GX_NSTAGE, e->stream), "qmeta reset");
+    CK(cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->stream), "err reset");
+    CK(cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 16, e->stream), "stats reset");
+
+    if (o.mode == GEGS_MODE_PERSISTENT) {
+        st = build_graph(e, grid, threads);
+        if (st != GEGS_OK) return st;
+        CK(cudaEventRecord(e->ev0, e->stream), "event");
+        k_plan<<<1, 1, 0, e->stream>>>(e->ctx, e->d_sched);
+        CK(cudaGraphLaunch(e->gexec, e->stream), "graph launch");
+        CK(cudaEventRecord(e->ev1, e->stream), "event");
+    } else {
+        // Plain form: host-driven, one kernel per event type, synchronise and
+        // read the queue counters back after every launch (CUDA_EGS.cu:226-365).
+        CK(cudaEventRecord(e->ev0, e->stream), "event");
+        uint32_t counts[GX_NSTAGE];
+        SchedState hsr;
+        for (uint32_t w = 0; w < max_waves; w++) {
+            k_plan<<<1, 1, 0, e->stream>>>(e->ctx, e->d_sched);
+            CK(cudaMemcpyAsync(&hsr, e->d_sched, sizeof hsr, cudaMemcpyDeviceToHost, e->stream), "sched D2H");
+            CK(cudaStreamSynchronize(e->stream), "plain sync");
+            if (!hsr.pending) break;
+            k_source<<<grid, threads, 0, e->stream>>>(e->ctx, e->d_sched);
+            const int order[GX_NSTAGE] = {ST_PHOTON, ST_COMPTON, ST_PHOTO, ST_RAYLEIGH, ST_PAIR,
+                                          ST_ELECTRON, ST_MOLLER, ST_BREMS, ST_BHABHA, ST_ANNIH};
+            for (int k = 0; k < GX_NSTAGE; k++) {
+                switch (order[k]) {
+                case ST_PHOTON: k_plain<ST_PHOTON><<<grid, threads, 0, e->stream>>>(e->ctx); break;
+                case ST_COMPTON: k_plain<ST_COMPTON><<<grid, threads, 0, e->stream>>>(e->ctx); break;
+                case ST_PHOTO: k_plain<ST_PHOTO><<<grid, threads, 0, e->stream>>>(e->ctx); break;
+                case ST_RAYLEIGH: k_plain<ST_RAYLEIGH><<<grid, threads, 0, e->stream>>>(e->ctx); break;
+                case ST_PAIR: k_plain<ST_PAIR><<<grid, threads, 0, e->stream>>>(e->ctx); break;
+                case ST_ELECTRON: k_plain<ST_ELECTRON><<<grid, threads, 0, e->stream>>>(e->ctx); break;
+                case ST_MOLLER: k_plain<ST_MOLLER><<<grid, threads, 0, e->stream>>>(e->ctx); break;
+                case ST_BREMS: k_plain<ST_BREMS><<<grid, threads, 0, e->stream>>>(e->ctx); break;
+                case ST_BHABHA: k_plain<ST_BHABHA><<<grid, threads, 0, e->stream>>>(e->ctx); break;
+                default: k_plain<ST_ANNIH><<<grid, threads, 0, e->stream>>>(e->ctx); break;
+                }
+                CK(cudaGetLastError(), "plain launch");
+                CK(cudaMemcpyAsync(counts, e->d_qmeta, sizeof counts, cudaMemcpyDeviceToHost, e->stream), "counts D2H");
+                CK(cudaStreamSynchronize(e->stream), "plain sync");
+            }
+        }
+        CK(cudaEventRecord(e->ev1, e->stream), "event");
+    }
+    CK(cudaGetLastError(), "launch");
+    CK(cudaStreamSynchronize(e->stream), "run sync");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    uint32_t errbits = 0;
+    unsigned long long stats[16];
+    SchedState hsr;
+    CK(cudaMemcpy(&errbits, e->d_err, sizeof errbits, cudaMemcpyDeviceToHost), "err D2H");
+    CK(cudaMemcpy(stats, e->d_stats, sizeof stats, cudaMemcpyDeviceToHost), "stats D2H");
+    CK(cudaMemcpy(&hsr, e->d_sched, sizeof hsr, cudaMemcpyDeviceToHost), "sched D2H");
+    gegs_run_stats &R = e->last;
+    for (int q = 0; q < GX_NSTAGE; q++) R.processed[q] = stats[q];
+    R.photon_steps = stats[GX_NSTAGE];
+    R.electron_steps = stats[GX_NSTAGE + 1];
+    R.waves = hsr.waves;
+    R.error_bits = errbits;
+    R.device_ms = ms;
+    if (errbits & GX_ERR_QUEUE_FULL) { e->err = "event queue overflow"; return GEGS_ERR_QUEUE_FULL; }
+    if (errbits & GX_ERR_MODULE) { e->err = "particle in an unsupported module"; return GEGS_ERR_MODULE; }
+    if (errbits & GX_ERR_SOURCE) { e->err = "history outside every field range"; return GEGS_ERR_SOURCE; }
+    if (errbits & GX_ERR_STEP_BUDGET) { e->err = "wave budget exhausted"; return GEGS_ERR_STEP_BUDGET; }
+    return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_get_tally(gegs_engine *e, int64_t *out, uint64_t nvox)
+{
+    if (!e || !out || nvox != e->nvox || !e->d_tally) return GEGS_ERR_ARG;
+    CK(cudaMemcpyAsync(out, e->d_tally, nvox * 8, cudaMemcpyDeviceToHost, e->stream), "tally D2H");
+    CK(cudaStreamSynchronize(e->stream), "tally sync");
+    return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_get_dose(gegs_engine *e, const float *voxel_mass, double dose_unit, double *out, uint64_t nvox)
+{
+    if (!e || !out || !voxel_mass || nvox != e->nvox || !e->d_tally) return GEGS_ERR_ARG;
+    float *d_mass = nullptr;
+    double *d_out = nullptr;
+    CK(cudaMallocAsync(&d_mass, nvox * 4, e->stream), "mass");
+    CK(cudaMallocAsync(&d_out, nvox * 8, e->stream), "dose");
+    CK(cudaMemcpyAsync(d_mass, voxel_mass, nvox * 4, cudaMemcpyHostToDevice, e->stream), "mass H2D");
+    k_dose<<<e->nsm * 4, 256, 0, e->stream>>>(e->d_tally, d_mass, dose_unit, d_out, nvox);
+    CK(cudaGetLastError(), "dose kernel");
+    CK(cudaMemcpyAsync(out, d_out, nvox * 8, cudaMemcpyDeviceToHost, e->stream), "dose D2H");
+    cudaFreeAsync(d_mass, e->stream);
+    cudaFreeAsync(d_out, e->stream);
+    CK(cudaStreamSynchronize(e->stream), "dose sync");
+    return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_set_trace(gegs_engine *e, uint32_t capacity)
+{
+    if (!e) return GEGS_ERR_ARG;
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    cudaFree(e->d_trace);
+    e->d_trace = nullptr;
+    if (!e->d_trace_n) CK(cudaMalloc(&e->d_trace_n, sizeof(uint32_t)), "trace counter");
+    CK(cudaMemset(e->d_trace_n, 0, sizeof(uint32_t)), "trace counter reset");
+    if (capacity) CK(cudaMalloc(&e->d_trace, (size_t)capacity * sizeof(TraceRec)), "trace buffer");
+    e->trace_cap = capacity;
+    e->ctx.trace = e->d_trace;
+    e->ctx.trace_n = e->d_trace_n;
+    e->ctx.trace_cap = capacity;
+    e->ctx_gen++;
+    return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_get_trace(gegs_engine *e, void *out, uint32_t capacity, uint32_t *n)
+{
+    if (!e || !n || !e->d_trace_n) return GEGS_ERR_ARG;
+    uint32_t cnt = 0;
+    CK(cudaMemcpy(&cnt, e->d_trace_n, sizeof cnt, cudaMemcpyDeviceToHost), "trace count");
+    *n = cnt;
+    uint32_t m = cnt < capacity ? cnt : capacity;
+    if (m > e->trace_cap) m = e->trace_cap;
+    if (m && out) CK(cudaMemcpy(out, e->d_trace, (size_t)m * sizeof(TraceRec), cudaMemcpyDeviceToHost), "trace D2H");
+    CK(cudaMemset(e->d_trace_n, 0, sizeof(uint32_t)), "trace counter reset");
+    return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_get_stats(gegs_engine *e, gegs_run_stats *out)
+{
+    if (!e || !out) return GEGS_ERR_ARG;
+    *out = e->last;
+    return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_tally_device_ptr(gegs_engine *e, void **out)
+{
+    if (!e || !out || !e->d_tally) return GEGS_ERR_ARG;
+    *out = e->d_tally;
+    return GEGS_OK;
+}

@@ -1,0 +1,290 @@
+// Transport kernels.  One consumer kernel per event queue (the reference's
+// ten stacks, CUDA_EGS.h:362-367), fed by a source kernel that turns
+// phase-space records into primaries on the device.
+//
+// Persistent form: the photon and electron consumers keep every lane busy by
+// refilling idle lanes from the queue with one warp-aggregated atomic per
+// refill (persistent threads with regeneration), and a one-thread planner
+// kernel decides the next wave and sets the CUDA-graph loop condition, so a
+// whole run is a single graph launch with no host round trip.
+// Plain form: the reference's structure -- each thread pops its own particle
+// with a global atomic, and the host synchronises and reads the queue counters
+// back after every launch (CUDA_EGS.cu:226-365, 498-799).
+#pragma once
+#include "dev_electron.cuh"
+
+// steps one particle may take inside one consumer launch before it is dropped
+// and GX_ERR_STEP_BUDGET is raised (guards the persistent loops against a
+// particle that stops making progress)
+#define GX_STEP_BUDGET 4000000u
+
+struct SchedState {
+    unsigned long long next, end;     // history cursor
+    unsigned long long h0, h1;        // histories injected by the current wave
+    uint32_t batch, waves, max_waves, pending;
+};
+
+__device__ __forceinline__ void consumer_done(const DevCtx &C, int q)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        uint32_t prev = atomicAdd(&C.q.done[q], 1u);
+        if (prev == gridDim.x - 1) {
+            C.q.count[q] = 0;
+            C.q.head[q] = 0;
+            C.q.done[q] = 0;
+            __threadfence();
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t queue_len(const DevCtx &C, int q)
+{
+    uint32_t n = *((volatile uint32_t *)&C.q.count[q]);
+    return n < C.q.cap[q] ? n : C.q.cap[q];
+}
+
+__device__ __forceinline__ void block_stat_add(const DevCtx &C, int slot, unsigned long long v)
+{
+    // warp reduction then one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&C.stats[slot], v);
+}
+
+// ---- source: history index -> primary (CUDA_EGS.cu:52-131) -----------------
+__device__ bool make_primary(const DevCtx &C, unsigned long long h, Part &p)
+{
+    int f;
+    for (f = 0; f < C.nfields; f++) {
+        unsigned long long hb = C.fields[f].hist_begin, he = C.fields[f].hist_end;
+        if (h >= hb && h < he) break;
+    }
+    if (f == C.nfields) return false;
+    const gegs_field *F = &C.fields[f];
+    unsigned long long j = (h - F->hist_begin) / (unsigned long long)(F->nrepeat + 1);
+    const gegs_phsp_record *rec = &C.phsp[j % C.nphsp];
+    uint32_t latch = __ldg(&rec->latch);
+    float re = __ldg(&rec->e), rx = __ldg(&rec->x), ry = __ldg(&rec->y);
+    float ru = __ldg(&rec->u), rv = __ldg(&rec->v), rwt = __ldg(&rec->wt);
+    int q;
+    if (latch & 0x40000000u) q = -1;
+    else if (latch & 0x20000000u) q = 1;
+    else q = 0;
+    float w2 = 1.0f - ru * ru - rv * rv;
+    float w = sqrtf(w2 > 0.0f ? w2 : 0.0f);
+    float wt = rwt;
+    if (wt < 0.0f) { w = -w; wt = -wt; }
+    p.charge = (int8_t)q;
+    p.e = re < 0.0f ? -re : re;
+    p.wt = wt;
+    p.region = 0;
+    p.leafIndex = GX_OUTMLC;
+    p.bank = -1;
+    p.module = (uint8_t)C.module_order[0];
+    p.field = (uint8_t)f;
+    p.x = rx; p.y = ry; p.z = C.z_phsp;
+    p.u = ru; p.v = rv; p.w = w;
+    p.hist_lo = (uint32_t)h;
+    p.hist_hi = (uint32_t)(h >> 32);
+    p.sid_lo = 0; p.sid_hi = 0; p.ctr = 0;
+    p.status = 0; p.pad0 = 0; p.pad1 = 0;
+    return true;
+}
+
+__global__ void k_source(const __grid_constant__ DevCtx C, const SchedState *st)
+{
+    unsigned long long h0 = st->h0, h1 = st->h1;
+    unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long h = h0 + blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; h < h1; h += stride) {
+        Part p;
+        if (!make_primary(C, h, p)) { atomicOr(C.err, GX_ERR_SOURCE); continue; }
+        push(C, p.charge == 0 ? ST_PHOTON : ST_ELECTRON, p);
+    }
+}
+
+// ---- persistent consumers with warp regeneration ---------------------------
+template <int Q>
+__device__ __forceinline__ bool refill(const DevCtx &C, uint32_t n, bool &exhausted, bool active, Part &p, Rng &r)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    unsigned need = __ballot_sync(0xffffffffu, !active);
+    if (need == 0u || exhausted) return active;
+    uint32_t cnt = __popc(need);
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&C.q.head[Q], cnt);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base + cnt >= n) exhausted = true;
+    if (!active) {
+        uint32_t idx = base + __popc(need & ((1u << lane) - 1u));
+        if (idx < n) {
+            p = load_part(&C.q.buf[Q][idx]);
+            rng_load(r, p);
+            trace_event(C, 1u, Q, p);
+            return true;
+        }
+    }
+    return active;
+}
+
+__global__ void __launch_bounds__(256) k_photon(const __grid_constant__ DevCtx C)
+{
+    const uint32_t n = queue_len(C, ST_PHOTON);
+    Part p;
+    Rng r;
+    bool active = false, exhausted = false;
+    unsigned long long taken = 0, steps = 0;
+    uint32_t nst = 0;
+    for (;;) {
+        bool was = active;
+        active = refill<ST_PHOTON>(C, n, exhausted, active, p, r);
+        if (active && !was) { taken++; nst = 0; }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active) {
+            steps++;
+            if (photon_step(C, p, r)) active = false;
+            else if (++nst > GX_STEP_BUDGET) { active = false; atomicOr(C.err, GX_ERR_STEP_BUDGET); }
+        }
+    }
+    block_stat_add(C, ST_PHOTON, taken);
+    block_stat_add(C, GX_NSTAGE, steps);
+    consumer_done(C, ST_PHOTON);
+}
+
+__global__ void __launch_bounds__(256) k_electron(const __grid_constant__ DevCtx C)
+{
+    const uint32_t n = queue_len(C, ST_ELECTRON);
+    Part p;
+    Rng r;
+    EState s;
+    bool active = false, exhausted = false;
+    unsigned long long taken = 0, steps = 0;
+    uint32_t nst = 0;
+    for (;;) {
+        bool was = active;
+        active = refill<ST_ELECTRON>(C, n, exhausted, active, p, r);
+        if (active && !was) { taken++; estate_init(s); nst = 0; }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (active) {
+            steps++;
+            if (electron_step(C, p, r, s)) active = false;
+            else if (++nst > GX_STEP_BUDGET) { active = false; atomicOr(C.err, GX_ERR_STEP_BUDGET); }
+        }
+    }
+    block_stat_add(C, ST_ELECTRON, taken);
+    block_stat_add(C, GX_NSTAGE + 1, steps);
+    consumer_done(C, ST_ELECTRON);
+}
+
+template <int Q>
+__device__ __forceinline__ void run_interaction(const DevCtx &C, const Part &p, Rng &r)
+{
+    if (Q == ST_COMPTON) compton(C, p, r);
+    else if (Q == ST_PHOTO) photo(C, p, r);
+    else if (Q == ST_RAYLEIGH) rayleigh(C, p, r);
+    else if (Q == ST_PAIR) pair(C, p, r);
+    else if (Q == ST_MOLLER) moller(C, p, r);
+    else if (Q == ST_BREMS) brems(C, p, r);
+    else if (Q == ST_BHABHA) bhabha(C, p, r);
+    else if (Q == ST_ANNIH) annih(C, p, r);
+}
+
+template <int Q>
+__global__ void __launch_bounds__(256) k_interact(const __grid_constant__ DevCtx C)
+{
+    const uint32_t n = queue_len(C, Q);
+    unsigned long long taken = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Part p = load_part(&C.q.buf[Q][i]);
+        Rng r;
+        rng_load(r, p);
+        trace_event(C, 1u, Q, p);
+        run_interaction<Q>(C, p, r);
+        taken++;
+    }
+    block_stat_add(C, Q, taken);
+    consumer_done(C, Q);
+}
+
+// ---- plain form: per-thread pops, one stage per launch ---------------------
+template <int Q>
+__global__ void __launch_bounds__(256) k_plain(const __grid_constant__ DevCtx C)
+{
+    const uint32_t n = queue_len(C, Q);
+    unsigned long long taken = 0, steps = 0;
+    for (;;) {
+        uint32_t idx = atomicAdd(&C.q.head[Q], 1u);
+        if (idx >= n) break;
+        Part p = load_part(&C.q.buf[Q][idx]);
+        Rng r;
+        rng_load(r, p);
+        trace_event(C, 1u, Q, p);
+        taken++;
+        if (Q == ST_PHOTON) {
+            uint32_t nst = 0;
+            while (!photon_step(C, p, r)) {
+                steps++;
+                if (++nst > GX_STEP_BUDGET) { atomicOr(C.err, GX_ERR_STEP_BUDGET); break; }
+            }
+            steps++;
+        } else if (Q == ST_ELECTRON) {
+            EState s;
+            estate_init(s);
+            uint32_t nst = 0;
+            while (!electron_step(C, p, r, s)) {
+                steps++;
+                if (++nst > GX_STEP_BUDGET) { atomicOr(C.err, GX_ERR_STEP_BUDGET); break; }
+            }
+            steps++;
+        } else {
+            run_interaction<Q>(C, p, r);
+        }
+    }
+    block_stat_add(C, Q, taken);
+    if (Q == ST_PHOTON) block_stat_add(C, GX_NSTAGE, steps);
+    if (Q == ST_ELECTRON) block_stat_add(C, GX_NSTAGE + 1, steps);
+    consumer_done(C, Q);
+}
+
+// ---- planner: next wave's injection and the loop condition -----------------
+__device__ __forceinline__ uint32_t plan_wave(const DevCtx &C, SchedState *st)
+{
+    uint32_t inflight = 0;
+    for (int q = 0; q < GX_NSTAGE; q++) inflight += *((volatile uint32_t *)&C.q.count[q]);
+    uint32_t main_q = *((volatile uint32_t *)&C.q.count[ST_PHOTON]) + *((volatile uint32_t *)&C.q.count[ST_ELECTRON]);
+    unsigned long long remaining = st->end - st->next;
+    unsigned long long inject = 0;
+    if (remaining > 0 && main_q < st->batch / 2) inject = remaining < st->batch ? remaining : st->batch;
+    st->h0 = st->next;
+    st->h1 = st->next + inject;
+    st->next += inject;
+    st->waves++;
+    uint32_t pending = (inflight > 0 || inject > 0 || st->next < st->end) ? 1u : 0u;
+    if (pending && st->waves >= st->max_waves) {
+        atomicOr(C.err, GX_ERR_STEP_BUDGET);
+        pending = 0;
+    }
+    if (*((volatile uint32_t *)C.err) & GX_ERR_QUEUE_FULL) pending = 0;
+    st->pending = pending;
+    return pending;
+}
+
+__global__ void k_plan(const __grid_constant__ DevCtx C, SchedState *st)
+{
+    plan_wave(C, st);
+}
+
+__global__ void k_plan_cond(const __grid_constant__ DevCtx C, SchedState *st, cudaGraphConditionalHandle handle)
+{
+    uint32_t pending = plan_wave(C, st);
+    cudaGraphSetConditional(handle, pending);
+}
+
+__global__ void k_dose(const unsigned long long *tally, const float *mass, double unit, double *out, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        double m = (double)mass[i];
+        if (m == 0.0) m = 1.0;
+        out[i] = (double)(long long)tally[i] * 9.313225746154785e-10 / m * unit;
+    }
+}

@@ -1,0 +1,164 @@
+"""ctypes binding of the C ABI (``include/gegs.h``) of ``libgegs_b200.so``.
+
+The CUDA library is the only compute path: if it cannot be loaded, or no GPU
+is visible, these calls raise -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+import numpy as np
+
+from .scene import PhspRecord
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "libgegs_b200.so"
+
+STATUS = {0: "GEGS_OK", 1: "GEGS_ERR_ARG", 2: "GEGS_ERR_CUDA", 3: "GEGS_ERR_QUEUE_FULL", 4: "GEGS_ERR_MODULE",
+          5: "GEGS_ERR_NOMEM", 6: "GEGS_ERR_STEP_BUDGET", 7: "GEGS_ERR_SOURCE"}
+MODE_PERSISTENT, MODE_PLAIN = 0, 1
+
+EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
+           "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_get_dose", "gegs_get_stats",
+           "gegs_tally_device_ptr", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version"]
+
+
+TRACE_DTYPE = np.dtype([("kind_stage", "<u4"), ("hist_lo", "<u4"), ("sid_lo", "<u4"), ("sid_hi", "<u4"),
+                        ("ctr", "<u4"), ("e", "<f4"), ("x", "<f4"), ("region", "<u4")])
+
+
+class GegsError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class RunOpts(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("batch", C.c_uint32), ("blocks_per_sm", C.c_int32),
+                ("threads_per_block", C.c_int32), ("max_waves", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("processed", C.c_uint64 * 10), ("photon_steps", C.c_uint64), ("electron_steps", C.c_uint64),
+                ("waves", C.c_uint32), ("error_bits", C.c_uint32), ("device_ms", C.c_double)]
+
+
+_lib = None
+
+
+def load_library(path=None):
+    """Load the CUDA library (raises OSError when it is missing)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    L = C.CDLL(str(path or LIB_PATH))
+    vp = C.c_void_p
+    L.gegs_create.argtypes = [C.c_int, C.POINTER(vp)]
+    L.gegs_destroy.argtypes = [vp]
+    L.gegs_destroy.restype = None
+    L.gegs_last_error.argtypes = [vp]
+    L.gegs_last_error.restype = C.c_char_p
+    L.gegs_set_physics.argtypes = [vp, vp]
+    L.gegs_set_scene.argtypes = [vp, vp]
+    L.gegs_set_phsp.argtypes = [vp, vp, C.c_uint64]
+    L.gegs_run.argtypes = [vp, C.c_uint64, C.c_uint64, C.POINTER(RunOpts)]
+    L.gegs_reset_tally.argtypes = [vp]
+    L.gegs_get_tally.argtypes = [vp, vp, C.c_uint64]
+    L.gegs_get_dose.argtypes = [vp, vp, C.c_double, vp, C.c_uint64]
+    L.gegs_get_stats.argtypes = [vp, C.POINTER(RunStats)]
+    L.gegs_tally_device_ptr.argtypes = [vp, C.POINTER(vp)]
+    L.gegs_set_trace.argtypes = [vp, C.c_uint32]
+    L.gegs_get_trace.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_uint32)]
+    for f in ("gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field"):
+        getattr(L, f).restype = C.c_size_t
+    L.gegs_version.restype = C.c_char_p
+    if path is None:
+        _lib = L
+    return L
+
+
+class Engine:
+    """One CUDA device + stream with the transport state (see include/gegs.h)."""
+
+    def __init__(self, device: int = 0):
+        self.L = load_library()
+        self.h = C.c_void_p()
+        st = self.L.gegs_create(device, C.byref(self.h))
+        if st != 0:
+            msg = self.L.gegs_last_error(self.h).decode() if self.h else "create failed"
+            if self.h:
+                self.L.gegs_destroy(self.h)
+                self.h = C.c_void_p()
+            raise GegsError(st, msg)
+        self.nvox = 0
+        self._keep = None
+
+    def _check(self, st):
+        if st != 0:
+            raise GegsError(st, self.L.gegs_last_error(self.h).decode())
+
+    def close(self):
+        if self.h:
+            self.L.gegs_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_physics(self, block: np.ndarray):
+        blk = np.ascontiguousarray(block)
+        assert blk.dtype.itemsize == self.L.gegs_sizeof_physics()
+        self._check(self.L.gegs_set_physics(self.h, blk.ctypes.data))
+
+    def set_scene(self, scene_holder):
+        self._keep = scene_holder
+        self._check(self.L.gegs_set_scene(self.h, C.addressof(scene_holder.scene)))
+        self.nvox = scene_holder.nvox
+
+    def set_phsp(self, recs: np.ndarray):
+        r = np.ascontiguousarray(recs)
+        self._check(self.L.gegs_set_phsp(self.h, r.ctypes.data, len(r)))
+
+    def run(self, h0: int, h1: int, mode: int = MODE_PERSISTENT, batch: int = 0, blocks_per_sm: int = 0,
+            threads: int = 0, max_waves: int = 0):
+        o = RunOpts(mode, batch, blocks_per_sm, threads, max_waves, 0)
+        self._check(self.L.gegs_run(self.h, h0, h1, C.byref(o)))
+        return self.stats()
+
+    def reset_tally(self):
+        self._check(self.L.gegs_reset_tally(self.h))
+
+    def tally(self) -> np.ndarray:
+        out = np.zeros(self.nvox, np.int64)
+        self._check(self.L.gegs_get_tally(self.h, out.ctypes.data, self.nvox))
+        return out
+
+    def dose(self, voxel_mass: np.ndarray, dose_unit: float = 1.6e-8) -> np.ndarray:
+        m = np.ascontiguousarray(voxel_mass, np.float32)
+        out = np.zeros(self.nvox, np.float64)
+        self._check(self.L.gegs_get_dose(self.h, m.ctypes.data, dose_unit, out.ctypes.data, self.nvox))
+        return out
+
+    def stats(self) -> dict:
+        s = RunStats()
+        self._check(self.L.gegs_get_stats(self.h, C.byref(s)))
+        return dict(processed=list(s.processed), photon_steps=s.photon_steps, electron_steps=s.electron_steps,
+                    waves=s.waves, error_bits=s.error_bits, device_ms=s.device_ms)
+
+    def set_trace(self, capacity: int):
+        self._check(self.L.gegs_set_trace(self.h, capacity))
+        self._trace_cap = capacity
+
+    def get_trace(self) -> np.ndarray:
+        buf = np.zeros(self._trace_cap, TRACE_DTYPE)
+        n = C.c_uint32()
+        self._check(self.L.gegs_get_trace(self.h, buf.ctypes.data, self._trace_cap, C.byref(n)))
+        return buf[:min(n.value, self._trace_cap)]
+
+    def tally_device_ptr(self) -> int:
+        p = C.c_void_p()
+        self._check(self.L.gegs_tally_device_ptr(self.h, C.byref(p)))
+        return p.value

@@ -4,12 +4,13 @@ The transport kernels read EGSnrc-style interpolation tables (log-linear
 ``a + b*ln(E)`` pairs, Rayleigh form-factor CDFs, Goudsmit-Saunderson
 multiple-scattering surfaces, shell/edge data).  In the reference these are
 ``__device__`` globals filled by HATCH (``commonBlocks dev.h:11-262``,
-``media.cu:96-100``).  Here they travel as ONE flat, 4-byte-aligned block
+``media.cu:96-100``).  Here they travel as ONE flat block
 whose field order is fixed by :data:`FIELDS`; ``include/gegs_physics.h`` is
 generated from the same list (see :func:`render_header`) so the C struct, the
 numpy structured dtype and the blob bytes always agree.
 
-Every field is float32 or int32, so the C struct has no padding and the
+Every field is float32 or int32 and every array starts on a 16-byte boundary
+(explicit ``_padN`` members), so the C struct has no compiler padding and the
 numpy dtype offsets equal the C ``offsetof`` values.
 
 Index conventions follow the reference exactly (e.g. ``gmfp[med*MXGE+lgle]``,
@@ -112,10 +113,27 @@ FIELDS = [
 ]
 
 
+def padded_fields():
+    """FIELDS with int32 padding so every array field starts on a 16-byte
+    boundary (the kernels read float2/float4 table entries with vector loads)."""
+    out, off, k = [], 0, 0
+    for name, kind, shape in FIELDS:
+        if shape and off % 16:
+            npad = (16 - off % 16) // 4
+            out.append((f"_pad{k}", I, (npad,)))
+            off += 4 * npad
+            k += 1
+        out.append((name, kind, shape))
+        off += 4 * int(np.prod(shape)) if shape else 4
+    if off % 16:
+        out.append((f"_pad{k}", I, ((16 - off % 16) // 4,)))
+    return out
+
+
 def dtype() -> np.dtype:
     """numpy structured dtype equal, byte for byte, to ``struct gegs_physics``."""
     parts = []
-    for name, kind, shape in FIELDS:
+    for name, kind, shape in padded_fields():
         base = np.float32 if kind == F else np.int32
         parts.append((name, base, shape) if shape else (name, base))
     dt = np.dtype(parts, align=False)
@@ -135,14 +153,15 @@ def render_header() -> str:
                " * Physics-table block read by the transport kernels.  Same content and\n"
                " * index conventions as the reference's __device__ globals\n"
                " * (commonBlocks dev.h:11-262, media.cu:96-100); float2 pairs are float[2].\n"
-               " * Every member is 4 bytes wide, so the struct has no padding. */\n")
+               " * Every member is 4 bytes wide; _padN members put every array on a\n"
+               " * 16-byte boundary so the kernels can use float2/float4 loads. */\n")
     out.append("#ifndef GEGS_PHYSICS_H\n#define GEGS_PHYSICS_H\n\n#include <stdint.h>\n\n")
     for k, v in CONSTANTS.items():
         out.append(f"#define GEGS_{k} {v}\n")
     out.append(f"#define GEGS_MS_SIZE {MS_SIZE}\n")
     out.append(f"#define GEGS_MAX_EII_BINS {MAX_EII_BINS}\n\n")
     out.append("typedef struct gegs_physics {\n")
-    for name, kind, shape in FIELDS:
+    for name, kind, shape in padded_fields():
         ctype = "float" if kind == F else "int32_t"
         dims = "".join(f"[{d}]" for d in shape)
         out.append(f"    {ctype} {name}{dims};\n")

@@ -1,0 +1,121 @@
+/* C ABI of the B200 transport library (libgegs_b200.so).
+ *
+ * Plain pointers and sizes only.  One engine = one CUDA device + one stream;
+ * an engine is not thread-safe (drive it from one host thread at a time).
+ * The caller owns host buffers; the engine owns its device buffers.
+ *
+ * Mapping to the reference (RicciWoo/GEGS), which is a monolithic program
+ * whose internal seams these calls replace:
+ *   gegs_create + gegs_set_physics + gegs_set_scene
+ *       replace init() (init.cu:1682-1710): tables, phantom, MLC/jaws set-up
+ *       and the cudaMemcpyToSymbol uploads (copy.cu:3-277).
+ *   gegs_run
+ *       replaces runSimulation(histories_per_MU, iField) (CUDA_EGS.cu:367-900)
+ *       and its per-kernel host loop launch_kernels() (CUDA_EGS.cu:226-365);
+ *       all fields of the scene run in one call.
+ *   gegs_get_tally / gegs_get_dose
+ *       replace the D2H copy of eng_score and the host field sum
+ *       (CUDA_EGS.cu:1723-1735) and the dose conversion of write_dose()
+ *       (output.c:873-918).
+ * Errors are returned as status codes; the reference calls exit() instead
+ * (output.c:51-90).
+ */
+#ifndef GEGS_H
+#define GEGS_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "gegs_physics.h"
+#include "gegs_scene.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gegs_engine gegs_engine;
+
+typedef enum gegs_status {
+    GEGS_OK = 0,
+    GEGS_ERR_ARG = 1,          /* invalid argument or call order */
+    GEGS_ERR_CUDA = 2,         /* CUDA runtime error (see gegs_last_error) */
+    GEGS_ERR_QUEUE_FULL = 3,   /* an event queue overflowed: particles were lost */
+    GEGS_ERR_MODULE = 4,       /* particle in an unsupported beam module */
+    GEGS_ERR_NOMEM = 5,        /* device allocation failed */
+    GEGS_ERR_STEP_BUDGET = 6,  /* the wave budget of a run was exhausted */
+    GEGS_ERR_SOURCE = 7        /* history outside every field's range */
+} gegs_status;
+
+typedef enum gegs_mode {
+    GEGS_MODE_PERSISTENT = 0,  /* device-driven wave loop in one CUDA graph */
+    GEGS_MODE_PLAIN = 1        /* host loop: one kernel per event type, sync + counter read-back each launch */
+} gegs_mode;
+
+typedef struct gegs_run_opts {
+    int32_t mode;              /* gegs_mode */
+    uint32_t batch;            /* histories kept in flight (0 = default) */
+    int32_t blocks_per_sm;     /* 0 = default */
+    int32_t threads_per_block; /* 0 = default */
+    uint32_t max_waves;        /* safety budget (0 = default) */
+    uint32_t reserved;
+} gegs_run_opts;
+
+typedef struct gegs_run_stats {
+    uint64_t processed[10];    /* particles handled per stage: photon, compton, photo, rayleigh,
+                                  pair, electron, moller, brems, bhabha, annih */
+    uint64_t photon_steps, electron_steps;
+    uint32_t waves;
+    uint32_t error_bits;
+    double device_ms;          /* device time of the last gegs_run (CUDA events) */
+} gegs_run_stats;
+
+/* Engine life cycle */
+gegs_status gegs_create(int device, gegs_engine **out);
+void gegs_destroy(gegs_engine *e);
+const char *gegs_last_error(const gegs_engine *e);
+
+/* Physics tables (struct gegs_physics, same layout the reference keeps in
+ * __device__ globals); copied to HBM. */
+gegs_status gegs_set_physics(gegs_engine *e, const gegs_physics *P);
+
+/* Phantom, beam-line geometry, fields and phase space; all copied to HBM.
+ * Resets the tally. */
+gegs_status gegs_set_scene(gegs_engine *e, const gegs_scene *S);
+
+/* Replace only the phase-space records (host memory; copied on the engine's stream). */
+gegs_status gegs_set_phsp(gegs_engine *e, const gegs_phsp_record *recs, uint64_t n);
+
+/* Transport histories [hist_begin, hist_end) of the scene; energy is added to
+ * the int64 tally (MeV * 2^30 per voxel).  opts may be NULL. */
+gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts);
+
+gegs_status gegs_reset_tally(gegs_engine *e);
+
+/* Copy the int64 tally (nvox entries) to host memory. */
+gegs_status gegs_get_tally(gegs_engine *e, int64_t *out, uint64_t nvox);
+
+/* dose[i] = tally[i] * 2^-30 / voxel_mass[i] * dose_unit, in double, on the device;
+ * voxel_mass is a host array of nvox entries (0 treated as 1, init.cu:1256-1271). */
+gegs_status gegs_get_dose(gegs_engine *e, const float *voxel_mass, double dose_unit, double *out, uint64_t nvox);
+
+gegs_status gegs_get_stats(gegs_engine *e, gegs_run_stats *out);
+
+/* Device pointer of the tally (for callers that keep results in HBM). */
+gegs_status gegs_tally_device_ptr(gegs_engine *e, void **out);
+
+/* Debug trace: record every queue push and every particle a consumer takes
+ * (32-byte records: kind|stage<<8, hist_lo, sid_lo, sid_hi, ctr, e, x, region).
+ * capacity 0 turns tracing off.  gegs_get_trace copies min(n, capacity)
+ * records, returns the number produced in *n and clears the buffer. */
+gegs_status gegs_set_trace(gegs_engine *e, uint32_t capacity);
+gegs_status gegs_get_trace(gegs_engine *e, void *out, uint32_t capacity, uint32_t *n);
+
+/* Library introspection */
+size_t gegs_sizeof_physics(void);
+size_t gegs_sizeof_scene(void);
+size_t gegs_sizeof_field(void);
+const char *gegs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GEGS_H */

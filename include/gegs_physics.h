@@ -3,7 +3,8 @@
  * Physics-table block read by the transport kernels.  Same content and
  * index conventions as the reference's __device__ globals
  * (commonBlocks dev.h:11-262, media.cu:96-100); float2 pairs are float[2].
- * Every member is 4 bytes wide, so the struct has no padding. */
+ * Every member is 4 bytes wide; _padN members put every array on a
+ * 16-byte boundary so the kernels can use float2/float4 loads. */
 #ifndef GEGS_PHYSICS_H
 #define GEGS_PHYSICS_H
 
@@ -45,25 +46,45 @@ typedef struct gegs_physics {
     int32_t iprdst;
     int32_t nbr_split;
     int32_t eii_flag;
+    int32_t _pad0[1];
     float rho[6];
+    int32_t _pad1[2];
     float ae[6];
+    int32_t _pad2[2];
     float ap[6];
+    int32_t _pad3[2];
     float ue[6];
+    int32_t _pad4[2];
     float up[6];
+    int32_t _pad5[2];
     float te[6];
+    int32_t _pad6[2];
     float thmoll[6];
+    int32_t _pad7[2];
     float rlc[6];
+    int32_t _pad8[2];
     float delcm[6];
+    int32_t _pad9[2];
     float zbrang[6];
+    int32_t _pad10[2];
     float lzbrang[6];
+    int32_t _pad11[2];
     float log_ap[6];
+    int32_t _pad12[2];
     float blcc[6];
+    int32_t _pad13[2];
     float xcc[6];
+    int32_t _pad14[2];
     float expeke1[6];
+    int32_t _pad15[2];
     float smaxir[6];
+    int32_t _pad16[2];
     float e_max_rr[6];
+    int32_t _pad17[2];
     int32_t i_do_rr[6];
+    int32_t _pad18[2];
     int32_t nne[6];
+    int32_t _pad19[2];
     float zelem[60];
     float pz[60];
     float wa[60];
@@ -103,11 +124,17 @@ typedef struct gegs_physics {
     float edge_d[1600];
     int32_t edge_number[100];
     int32_t iz_array[1538];
+    int32_t _pad20[2];
     int32_t shn_array[1538];
+    int32_t _pad21[2];
     int32_t ne_array[1538];
+    int32_t _pad22[2];
     float be_array[1538];
+    int32_t _pad23[2];
     float jo_array[1538];
+    int32_t _pad24[2];
     float erfjo_array[1538];
+    int32_t _pad25[2];
     int32_t shell_array[300];
     float eno_array[300];
     int32_t eno_atbin_array[300];
@@ -124,11 +151,13 @@ typedef struct gegs_physics {
     int32_t ims_array[16384];
     float eii_xsection[10000][2];
     float eii_cons[6];
+    int32_t _pad26[2];
     float eii[40][2];
     int32_t eii_z[40];
     int32_t eii_sh[40];
     int32_t eii_nshells[100];
     int32_t eii_nsh[6];
+    int32_t _pad27[2];
     int32_t eii_first[60];
     int32_t eii_no[60];
 } gegs_physics;

@@ -23,6 +23,10 @@ float ora_exp(float x);
 void ora_sincos_turns(float t, float *s, float *c);
 uint32_t ora_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, int lane);
 
+/* Debug trace of pushes (kind 0) and consumed particles (kind 1); forces one thread. */
+void ora_set_trace(void *buf, uint32_t cap);
+uint32_t ora_trace_count(void);
+
 /* Run histories [h0, h1); adds the int64 energy tally (MeV * 2^30) into `tally`. */
 int ora_run(const gegs_physics *P, const gegs_scene *S, uint64_t h0, uint64_t h1, int nthreads,
             int64_t *tally, ora_stats *stats);

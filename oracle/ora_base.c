@@ -152,8 +152,20 @@ void ora_escore(ora_ctx *C, uint32_t region, float energy)
     C->tally[region - VAC_AND_OTH] += (int64_t)llrintf(energy * 1073741824.0f);
 }
 
+void ora_trace(ora_ctx *C, uint32_t kind, int stage, const ora_particle *p)
+{
+    if (!C->trace) return;
+    uint32_t i = C->trace_n++;
+    if (i >= C->trace_cap) return;
+    ora_trace_rec *t = &C->trace[i];
+    t->kind_stage = kind | ((uint32_t)stage << 8);
+    t->hist_lo = p->rng.hist_lo; t->sid_lo = p->rng.sid_lo; t->sid_hi = p->rng.sid_hi; t->ctr = p->rng.ctr;
+    t->e = p->e; t->x = p->x; t->region = p->region;
+}
+
 void ora_push(ora_ctx *C, const ora_particle *p, int status)
 {
+    ora_trace(C, 0u, status, p);
     ora_stack *s = C->stk;
     if (s->n == s->cap) {
         s->cap = s->cap ? 2 * s->cap : 256;

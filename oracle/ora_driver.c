@@ -91,6 +91,7 @@ static int make_primary(const gegs_scene *S, uint64_t h, ora_particle *p)
 static void run_particle(ora_ctx *C, ora_particle *p)
 {
     C->counts[p->status]++;
+    ora_trace(C, 1u, p->status, p);
     switch (p->status) {
     case p_photon_step: ora_photon(C, p); break;
     case p_compton: ora_compton(C, p); break;
@@ -106,9 +107,16 @@ static void run_particle(ora_ctx *C, ora_particle *p)
     }
 }
 
+static ora_trace_rec *g_trace;
+static uint32_t g_trace_cap, g_trace_n;
+
+void ora_set_trace(void *buf, uint32_t cap) { g_trace = (ora_trace_rec *)buf; g_trace_cap = cap; g_trace_n = 0; }
+uint32_t ora_trace_count(void) { return g_trace_n; }
+
 int ora_run(const gegs_physics *P, const gegs_scene *S, uint64_t h0, uint64_t h1, int nthreads,
             int64_t *tally, ora_stats *stats)
 {
+    if (g_trace) nthreads = 1;
     uint32_t nvox = (uint32_t)S->nx * (uint32_t)S->ny * (uint32_t)S->nz;
     ora_region *reg = build_regions(P, S, nvox);
     ora_stats tot;
@@ -131,6 +139,9 @@ int ora_run(const gegs_physics *P, const gegs_scene *S, uint64_t h0, uint64_t h1
         C.seed_lo = (uint32_t)S->seed;
         C.seed_hi = (uint32_t)(S->seed >> 32);
         C.stk = &stk;
+        C.trace = g_trace;
+        C.trace_cap = g_trace_cap;
+        C.trace_n = g_trace_n;
         int64_t *loc = (int64_t *)calloc(nvox, sizeof(int64_t));
         C.tally = loc;
 #pragma omp for schedule(dynamic, 64)
@@ -152,6 +163,7 @@ int ora_run(const gegs_physics *P, const gegs_scene *S, uint64_t h0, uint64_t h1
             tot.steps_electron += C.steps_electron;
             tot.e_escaped += C.e_escaped;
             err |= C.error;
+            if (g_trace) g_trace_n = C.trace_n;
         }
         free(loc);
         free(stk.a);

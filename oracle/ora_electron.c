@@ -250,7 +250,12 @@ static float compute_eloss(const gegs_physics *P, int qel, unsigned medium, floa
 static void e_discard_below_cut(ora_ctx *C, ora_particle *p, const ora_region *rd)
 {
     ora_escore(C, p->region, (p->e - C->P->prm) * p->wt);
-    if (p->charge > 0) ora_annih_at_rest(C, p, rd, &p->rng);
+    if (p->charge > 0) {
+        /* the annihilation photons are spawned from the positron's stream: keep
+         * that stream in its own variable, the spawns overwrite p->rng */
+        ora_rng r = p->rng;
+        ora_annih_at_rest(C, p, rd, &r);
+    }
 }
 
 void ora_electron(ora_ctx *C, ora_particle *p)

@@ -103,6 +103,12 @@ typedef struct {
 } ora_stack;
 
 typedef struct {
+    uint32_t kind_stage, hist_lo, sid_lo, sid_hi, ctr;
+    float e, x;
+    uint32_t region;
+} ora_trace_rec;
+
+typedef struct {
     const gegs_physics *P;
     const gegs_scene *S;
     ora_region *reg;         /* nvox + 6 */
@@ -114,7 +120,11 @@ typedef struct {
     uint64_t steps_photon, steps_electron;
     double e_escaped;        /* energy leaving through region 0 (for conservation audits) */
     int error;
+    ora_trace_rec *trace;    /* debug trace (single-threaded runs only) */
+    uint32_t trace_n, trace_cap;
 } ora_ctx;
+
+void ora_trace(ora_ctx *C, uint32_t kind, int stage, const ora_particle *p);
 
 /* rng + math (ora_base.c) */
 uint32_t ora_philox_word(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, int lane);

@@ -51,8 +51,27 @@ def lib():
         L.ora_run.restype = C.c_int
         L.ora_run.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint64, C.c_int,
                               C.POINTER(C.c_int64), C.POINTER(Stats)]
+        L.ora_set_trace.argtypes = [C.c_void_p, C.c_uint32]
+        L.ora_trace_count.restype = C.c_uint32
         _lib = L
     return _lib
+
+
+TRACE_DTYPE = np.dtype([("kind_stage", "<u4"), ("hist_lo", "<u4"), ("sid_lo", "<u4"), ("sid_hi", "<u4"),
+                        ("ctr", "<u4"), ("e", "<f4"), ("x", "<f4"), ("region", "<u4")])
+
+
+def run_traced(physics, scene_holder, h0, h1, cap=1 << 20):
+    """Single-threaded run that also returns the push/consume trace."""
+    L = lib()
+    buf = np.zeros(cap, TRACE_DTYPE)
+    L.ora_set_trace(buf.ctypes.data, cap)
+    try:
+        tally, st = run(physics, scene_holder, h0, h1, threads=1)
+        n = L.ora_trace_count()
+    finally:
+        L.ora_set_trace(None, 0)
+    return tally, st, buf[:min(n, cap)]
 
 
 def run(physics: np.ndarray, scene_holder, h0: int, h1: int, threads: int = 0):

@@ -1,0 +1,46 @@
+"""The C-ABI library loads on a machine without a GPU and exports every
+symbol include/gegs.h declares; struct sizes agree with the Python mirrors."""
+import ctypes as C
+import re
+from pathlib import Path
+
+from gegs_b200 import build as B
+from gegs_b200 import engine as E
+from gegs_b200 import physics_layout as L
+from gegs_b200 import scene as S
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    txt = (ROOT / "include" / "gegs.h").read_text()
+    return sorted(set(re.findall(r"\b(gegs_[a-z_]+)\s*\(", txt)))
+
+
+def test_library_exports_all_declared_symbols():
+    B.build()
+    lib = E.load_library()
+    names = declared_functions()
+    assert set(E.EXPORTS) <= set(names)
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_sizes_match():
+    lib = E.load_library()
+    assert lib.gegs_sizeof_physics() == L.dtype().itemsize
+    assert lib.gegs_sizeof_scene() == C.sizeof(S.Scene)
+    assert lib.gegs_sizeof_field() == C.sizeof(S.Field)
+    assert lib.gegs_version().startswith(b"gegs_b200")
+
+
+def test_create_without_gpu_reports_error_not_crash():
+    import torch
+    if torch.cuda.is_available():
+        return
+    try:
+        E.Engine(0)
+    except E.GegsError as err:
+        assert err.status == 2
+    else:
+        raise AssertionError("engine creation must fail loudly without a GPU")
