@@ -1,0 +1,359 @@
+"""Benchmark: histories/s of the transport hot path on the synthetic CT head
+5-field plan (C3: 256x256x120 HU volume, 5 coplanar fields through jaws and a
+120-leaf MLC, 6 MV-like phase space), one JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gegs|reference]
+
+A step transports one batch of ``--hist-per-step`` histories.  ``value`` is
+the device-timed throughput (CUDA events on the engine stream) with every
+input resident in HBM; ``e2e`` repeats the steps through the C ABI from host
+memory: H2D of the step's phase-space records, the run, and D2H of the int64
+dose tally.  Multi-GPU (torchrun): each rank transports its own history range
+(weak scaling); the tallies are summed with one NCCL all-reduce.
+``--impl reference`` times the CPU restatement of the reference's routines
+(the oracle; the reference itself is CUDA-only and does not build here) on
+all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import re
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+MEASURED = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+METRIC = "histories/s (CT head 5-field plan, C3)"
+
+
+def hbm_peak():
+    try:
+        d = json.loads(MEASURED.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks + throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def traffic_from_profile(kind):
+    """DRAM bytes per launch of one kernel (scaled to the bench's launch size)
+    from the committed ncu summary ``profiles/<kind>_kernel_c3.md``."""
+    p = ROOT / "profiles" / f"{kind}_kernel_c3.md"
+    if not p.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+def algorithmic_bytes(job, sample):
+    """Per-history algorithmic bytes by stage, counted by the oracle on `sample` histories:
+    16 B per region record read, 16 B per tally update (8 B read + 8 B write),
+    8 B per float2 table read, 28 B per phase-space record (photon stage)."""
+    from oracle import oracle as O
+    sh = job.scene()
+    _, st = O.run(job.physics, sh, 0, sample)
+    cnt = np.array(st["cnt"], np.float64)
+    per_stage = (16 * cnt[:, 0] + 16 * cnt[:, 1] + 8 * cnt[:, 2]) / sample
+    per_stage[0] += 28.0
+    return per_stage, st
+
+
+def cpu_histories_per_s(job, seconds=15.0, threads=None):
+    """Oracle throughput on the host cores over a bounded sample (~`seconds`)."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count()
+    sh = job.scene()
+    n = 2000
+    t = time.perf_counter()
+    O.run(job.physics, sh, 0, n, threads=threads)
+    dt = time.perf_counter() - t
+    n2 = int(max(n, min(2_000_000, n * seconds / max(dt, 1e-3))))
+    t = time.perf_counter()
+    O.run(job.physics, sh, 0, n2, threads=threads)
+    dt = time.perf_counter() - t
+    return n2 / dt, n2, dt, threads
+
+
+def make_job(args, histories):
+    from gegs_b200 import workloads as W
+    return W.config3(histories=histories, nphsp=args.nphsp)
+
+
+def run_reference(args):
+    """CPU restatement of the reference routines (the oracle) on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    O.build()
+    job = make_job(args, 200_000_000)
+    rate, n, dt, cores = cpu_histories_per_s(job, seconds=args.ref_seconds)
+    per_step_ms = []
+    sh = job.scene()
+    steps_hist = n
+    for s in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        O.run(job.physics, sh, s * steps_hist, (s + 1) * steps_hist, threads=cores)
+        if s >= args.warmup:
+            per_step_ms.append((time.perf_counter() - t) * 1e3)
+    value = steps_hist * args.steps / (sum(per_step_ms) / 1e3)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(per_step_ms)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "C3 synthetic CT head 256x256x120, 5 fields, jaws +-6 cm, 120-leaf MLC, 6 MV-like phsp",
+                   "hist_per_step": steps_hist, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "histories/s", "cores": cores, "kind": "port",
+                         "sample": f"{steps_hist} C3 histories per step on {cores} threads (CPU restatement of the "
+                                   f"reference routines; the reference is CUDA-only and unbuildable here)"},
+        "e2e": {"value": value, "unit": "histories/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gegs", choices=["gegs", "reference"])
+    ap.add_argument("--hist-per-step", type=int, default=2_000_000)
+    ap.add_argument("--nphsp", type=int, default=10_000_000)
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--mode", default="persistent", choices=["persistent", "plain", "timed"],
+                    help="timed: the persistent form's kernels launched wave by wave from the host "
+                         "(per-kernel events; for ncu launch lists, which cannot see into the graph)")
+    ap.add_argument("--photon-budget", type=int, default=0)
+    ap.add_argument("--electron-budget", type=int, default=0)
+    ap.add_argument("--ref-seconds", type=float, default=8.0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    from gegs_b200 import build as B
+    B.build()
+    from gegs_b200.engine import MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED, Engine
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    H = args.hist_per_step
+    total = H * (args.warmup + args.steps) * world
+    job = make_job(args, max(total, 200_000_000))
+    sh = job.scene()
+    mode = {"persistent": MODE_PERSISTENT, "plain": MODE_PLAIN, "timed": MODE_TIMED}[args.mode]
+    ropt = dict(mode=mode, batch=args.batch, photon_budget=args.photon_budget, electron_budget=args.electron_budget)
+    eng = Engine(local)
+    eng.set_physics(job.physics)
+    eng.set_scene(sh)
+
+    def hist_range(step):
+        base = (rank * (args.warmup + args.steps) + step) * H
+        return base, base + H
+
+    for s in range(args.warmup):
+        eng.run(*hist_range(s), **ropt)
+    eng.reset_tally()
+
+    if dist is not None:
+        import torch
+        dist.barrier()
+        torch.cuda.synchronize()
+    dev_ms = []
+    stats = []
+    snaps = []
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for s in range(args.warmup, args.warmup + args.steps):
+            st = eng.run(*hist_range(s), **ropt)
+            dev_ms.append(st["device_ms"])
+            stats.append(st)
+            snaps.append(eng.tally())
+        if dist is not None:
+            import torch
+
+            class _Dev:
+                def __init__(self, ptr, n):
+                    self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i8", "data": (ptr, False),
+                                                     "version": 3}
+            t_dev = torch.as_tensor(_Dev(eng.tally_device_ptr(), eng.nvox), device=f"cuda:{local}")
+            dist.all_reduce(t_dev)
+            torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    elapsed_s = sum(dev_ms) / 1e3
+    if dist is not None:
+        import torch
+        tt = torch.tensor([elapsed_s, wall], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed_s, wall = float(tt[0]), float(tt[1])
+    value = H * args.steps * world / elapsed_s
+
+    # ---- end to end through the C ABI from host buffers -------------------
+    rec_per_step = int(np.ceil(H / (job.fields[0]["nrepeat"] + 1)))
+    e2e_ms = []
+    try:
+        import torch
+        pinned = torch.empty((rec_per_step * 28,), dtype=torch.uint8).pin_memory().numpy()
+    except Exception:
+        pinned = np.empty(rec_per_step * 28, np.uint8)
+    from gegs_b200.scene import PHSP_DTYPE
+    chunk = pinned.view(PHSP_DTYPE)
+    host_tally = np.empty(eng.nvox, np.int64)
+    for s in range(args.steps):
+        j0 = (s * rec_per_step) % max(1, len(job.phsp) - rec_per_step)
+        chunk[:] = job.phsp[j0:j0 + rec_per_step]
+        t = time.perf_counter()
+        eng.set_phsp(chunk)
+        eng.run(*hist_range(args.warmup + s), **ropt)
+        host_tally[:] = eng.tally()
+        e2e_ms.append((time.perf_counter() - t) * 1e3)
+    e2e = H * args.steps * world / (sum(e2e_ms) / 1e3)
+    if dist is not None:
+        import torch
+        tt = torch.tensor([sum(e2e_ms)], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e = H * args.steps * world / (float(tt[0]) / 1e3)
+
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant kernel (timed mode, outside the timed region)
+    eng.set_phsp(job.phsp)
+    tst = eng.run(0, H // 4, **dict(ropt, mode=MODE_TIMED))
+    kinds = ["photon", "compton", "photo", "rayleigh", "pair", "electron", "moller", "brems", "bhabha", "annih",
+             "source", "planner"]
+    share = np.array(tst["stage_ms"][:12])
+    dom = int(np.argmax(share[:10]))
+    launches = max(1, tst["stage_launches"][dom])
+    per_stage_bytes, ost = algorithmic_bytes(job, sample=20000)
+    alg_bytes_per_launch = per_stage_bytes[dom] * (H // 4) / launches
+    avg_launch_s = tst["stage_ms"][dom] / 1e3 / launches
+    peak, peak_kind = hbm_peak()
+    achieved = alg_bytes_per_launch / avg_launch_s / 1e9
+    tr = traffic_from_profile(kinds[dom])
+
+    # ---- batch-method statistical uncertainty -> time to 1 % ----------------
+    sig = None
+    if args.steps >= 3:
+        x = np.diff(np.concatenate([np.zeros((1, eng.nvox), np.int64), np.stack(snaps)]), axis=0).astype(np.float64)
+        mean = x.mean(axis=0)
+        sel = mean > 0.5 * mean.max()
+        se = x[:, sel].std(axis=0, ddof=1) / np.sqrt(x.shape[0])
+        rel = float(np.mean(se / mean[sel]))
+        sig = rel
+    t1pct = None
+    if sig:
+        n_done = H * args.steps * world
+        t1pct = (n_done * (sig / 0.01) ** 2) / value
+
+    cpu = None
+    if not args.no_cpu:
+        crate, cn, cdt, cores = cpu_histories_per_s(job, seconds=args.cpu_seconds)
+        cpu = {"value": crate, "unit": "histories/s", "cores": cores, "kind": "port",
+               "sample": f"{cn} C3 histories in {cdt:.1f} s on {cores} host threads (CPU oracle, same inputs)"}
+    # per step: the first planner launch, then per wave the source, 10 stage kernels and the planner
+    launches_per_step = [1 + 12 * (st["waves"] - 1) for st in stats]
+    line = {
+        "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed_s * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "C3 synthetic CT head 256x256x120 (1x1x2.5 mm), 5 coplanar fields 0/72/144/216/288 deg, "
+                               "jaws +-6 cm, 120-leaf MLC with seeded tips, 6 MV-like phase space "
+                               f"({len(job.phsp)} records, recycled)",
+                   "hist_per_step": H, "mode": args.mode, "parallelism": f"histories sharded over {world} GPU(s)",
+                   "l2": "working set (63 MB region table + 63 MB int64 tally + event queues) exceeds the 126 MB L2; no flush"},
+        "e2e": {"value": e2e, "unit": "histories/s", "h2d_bytes_per_step": rec_per_step * 28,
+                "d2h_bytes_per_step": eng.nvox * 8},
+        "roofline": {"bound": "hbm", "kernel": kinds[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": tr,
+                     "alg_bytes_per_launch": alg_bytes_per_launch, "avg_launch_ms": avg_launch_s * 1e3,
+                     "kernel_share": {k: float(v / share[:11].sum()) for k, v in zip(kinds[:11], share[:11])}},
+        "cpu_baseline": cpu,
+        "gpu_launches": int(sum(launches_per_step)),
+        "clocks": clk.summary(),
+        "stat_uncertainty": {"mean_rel_se_above_50pct_dmax": sig, "batches": args.steps,
+                             "time_to_1pct_s": t1pct},
+        "device_stats": {"processed": stats[-1]["processed"], "photon_steps": stats[-1]["photon_steps"],
+                         "electron_steps": stats[-1]["electron_steps"], "waves": stats[-1]["waves"]},
+        "wall_s": wall,
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

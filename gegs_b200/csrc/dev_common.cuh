@@ -40,6 +40,11 @@ static_assert(sizeof(gegs_field) % 16 == 0, "field record size");
 #define GX_MXGE GEGS_MXGE
 #define GX_MXEKE GEGS_MXEKE
 #define GX_NSTAGE 10
+// queues: 10 event stages, then ping-pong continuation queues for photons
+// (10, 11) and electrons (12, 13) that a budget-limited consumer re-queues into
+#define GX_Q_PCONT 10
+#define GX_Q_ECONT 12
+#define GX_NQ 14
 #define GX_LOOP_CAP 1000
 #define GX_EPSGMFP 1.e-5f
 #define GX_EPSEMFP 1.e-5f
@@ -88,12 +93,21 @@ struct TraceRec {
     uint32_t region;
 };
 
+// electron step state carried by a continued electron (EState, packed)
+struct __align__(16) EStatePk {
+    float elke, demfp, sig0, total_tstep;
+    int lelke;
+    uint32_t flags;       // bit0 compute_tstep, bit1 is_tstep
+    uint32_t pad0, pad1;
+};
+
 struct QueueSet {
-    Part *buf[GX_NSTAGE];
-    uint32_t cap[GX_NSTAGE];
-    uint32_t *count;      // [GX_NSTAGE] items queued
-    uint32_t *head;       // [GX_NSTAGE] items taken by the running consumer
-    uint32_t *done;       // [GX_NSTAGE] finished blocks of the running consumer
+    Part *buf[GX_NQ];
+    uint32_t cap[GX_NQ];
+    EStatePk *estate[2];  // state of the two electron continuation queues
+    uint32_t *count;      // [GX_NQ] items queued
+    uint32_t *head;       // [GX_NQ] items taken by the running consumer
+    uint32_t *done;       // [GX_NQ] finished blocks of the running consumer
 };
 
 // Everything a transport kernel needs; passed by value as a kernel parameter.
@@ -110,6 +124,8 @@ struct DevCtx {
     TraceRec *trace;                // debug trace (null = off)
     uint32_t *trace_n;
     uint32_t trace_cap;
+    const uint32_t *wave;           // wave counter (parity selects the continuation buffers)
+    uint32_t photon_budget, electron_budget;   // steps per particle per launch before continuation
     QueueSet q;
     uint64_t nphsp;
     int nx, ny, nz, nfields;

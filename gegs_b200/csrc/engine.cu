@@ -11,7 +11,7 @@
 namespace {
 
 // queue capacity per history in flight, per stage
-const float kCapFactor[GX_NSTAGE] = {6.f, 3.f, 3.f, 3.f, 3.f, 6.f, 3.f, 3.f, 3.f, 3.f};
+const float kCapFactor[GX_NQ] = {6.f, 3.f, 3.f, 3.f, 3.f, 6.f, 3.f, 3.f, 3.f, 3.f, 6.f, 6.f, 6.f, 6.f};
 
 }  // namespace
 
@@ -37,9 +37,10 @@ struct gegs_engine {
     TraceRec *d_trace = nullptr;
     uint32_t *d_trace_n = nullptr;
     uint32_t trace_cap = 0;
-    uint32_t *d_qmeta = nullptr;       // count[10], head[10], done[10]
-    Part *d_qbuf[GX_NSTAGE] = {};
-    uint32_t qcap[GX_NSTAGE] = {};
+    uint32_t *d_qmeta = nullptr;       // count[GX_NQ], head[GX_NQ], done[GX_NQ]
+    Part *d_qbuf[GX_NQ] = {};
+    EStatePk *d_estate[2] = {};
+    uint32_t qcap[GX_NQ] = {};
     uint32_t batch = 0;
 
     DevCtx ctx{};
@@ -101,8 +102,8 @@ gegs_status gegs_create(int device, gegs_engine **out)
     CK(cudaMalloc(&e->d_err, sizeof(uint32_t)), "err");
     CK(cudaMalloc(&e->d_stats, sizeof(unsigned long long) * 16), "stats");
     CK(cudaMalloc(&e->d_sched, sizeof(SchedState)), "sched");
-    CK(cudaMalloc(&e->d_qmeta, sizeof(uint32_t) * 3 * GX_NSTAGE), "qmeta");
-    CK(cudaMemset(e->d_qmeta, 0, sizeof(uint32_t) * 3 * GX_NSTAGE), "qmeta");
+    CK(cudaMalloc(&e->d_qmeta, sizeof(uint32_t) * 3 * GX_NQ), "qmeta");
+    CK(cudaMemset(e->d_qmeta, 0, sizeof(uint32_t) * 3 * GX_NQ), "qmeta");
     *out = e;
     return GEGS_OK;
 }
@@ -117,7 +118,8 @@ void gegs_destroy(gegs_engine *e)
     cudaFree(e->d_fields); cudaFree(e->d_cross); cudaFree(e->d_phsp); cudaFree(e->d_tally);
     cudaFree(e->d_err); cudaFree(e->d_stats); cudaFree(e->d_sched); cudaFree(e->d_qmeta);
     cudaFree(e->d_trace); cudaFree(e->d_trace_n);
-    for (int q = 0; q < GX_NSTAGE; q++) cudaFree(e->d_qbuf[q]);
+    for (int q = 0; q < GX_NQ; q++) cudaFree(e->d_qbuf[q]);
+    cudaFree(e->d_estate[0]); cudaFree(e->d_estate[1]);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -247,12 +249,13 @@ gegs_status gegs_reset_tally(gegs_engine *e)
 static gegs_status ensure_queues(gegs_engine *e, uint32_t batch)
 {
     if (batch == e->batch) return GEGS_OK;
-    for (int q = 0; q < GX_NSTAGE; q++) {
+    for (int q = 0; q < GX_NQ; q++) {
         uint64_t cap = (uint64_t)(kCapFactor[q] * (float)batch) + 4096;
         if (cap > 0xFFFFFFF0ull) cap = 0xFFFFFFF0ull;
         CK(realloc_dev(&e->d_qbuf[q], (size_t)cap), "queue buffer");
         e->qcap[q] = (uint32_t)cap;
     }
+    for (int k = 0; k < 2; k++) CK(realloc_dev(&e->d_estate[k], (size_t)e->qcap[GX_Q_ECONT + k]), "electron state");
     e->batch = batch;
     e->ctx_gen++;
     return GEGS_OK;
@@ -261,10 +264,13 @@ static gegs_status ensure_queues(gegs_engine *e, uint32_t batch)
 static void fill_queue_ctx(gegs_engine *e)
 {
     QueueSet &Q = e->ctx.q;
-    for (int q = 0; q < GX_NSTAGE; q++) { Q.buf[q] = e->d_qbuf[q]; Q.cap[q] = e->qcap[q]; }
+    for (int q = 0; q < GX_NQ; q++) { Q.buf[q] = e->d_qbuf[q]; Q.cap[q] = e->qcap[q]; }
+    Q.estate[0] = e->d_estate[0];
+    Q.estate[1] = e->d_estate[1];
     Q.count = e->d_qmeta;
-    Q.head = e->d_qmeta + GX_NSTAGE;
-    Q.done = e->d_qmeta + 2 * GX_NSTAGE;
+    Q.head = e->d_qmeta + GX_NQ;
+    Q.done = e->d_qmeta + 2 * GX_NQ;
+    e->ctx.wave = &e->d_sched->waves;
 }
 
 static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
@@ -319,11 +325,18 @@ extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hi
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     gegs_run_opts o = {};
     if (opts) o = *opts;
-    uint32_t batch = o.batch ? o.batch : (1u << 18);
+    uint32_t batch = o.batch ? o.batch : (1u << 19);
     int threads = o.threads_per_block ? o.threads_per_block : 256;
     int bps = o.blocks_per_sm ? o.blocks_per_sm : 4;
     int grid = e->nsm * bps;
     uint32_t max_waves = o.max_waves ? o.max_waves : 200000u;
+    uint32_t pb = (o.step_budget & 0xFFFFu) ? (o.step_budget & 0xFFFFu) : 32u;
+    uint32_t eb = (o.step_budget >> 16) ? (o.step_budget >> 16) : 16u;
+    if (pb != e->ctx.photon_budget || eb != e->ctx.electron_budget) {
+        e->ctx.photon_budget = pb;
+        e->ctx.electron_budget = eb;
+        e->ctx_gen++;
+    }
     gegs_status st = ensure_queues(e, batch);
     if (st != GEGS_OK) return st;
     fill_queue_ctx(e);
@@ -334,10 +347,11 @@ extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hi
     hs.batch = batch;
     hs.max_waves = max_waves;
     CK(cudaMemcpyAsync(e->d_sched, &hs, sizeof hs, cudaMemcpyHostToDevice, e->stream), "sched H2D");
-    CK(cudaMemsetAsync(e->d_qmeta, 0, sizeof(uint32_t) * 3 * GX_NSTAGE, e->stream), "qmeta reset");
+    CK(cudaMemsetAsync(e->d_qmeta, 0, sizeof(uint32_t) * 3 * GX_NQ, e->stream), "qmeta reset");
     CK(cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->stream), "err reset");
     CK(cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 16, e->stream), "stats reset");
 
+    for (int k = 0; k < 12; k++) { e->last.stage_ms[k] = 0.0; e->last.stage_launches[k] = 0; }
     if (o.mode == GEGS_MODE_PERSISTENT) {
         st = build_graph(e, grid, threads);
         if (st != GEGS_OK) return st;
@@ -345,11 +359,62 @@ extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hi
         k_plan<<<1, 1, 0, e->stream>>>(e->ctx, e->d_sched);
         CK(cudaGraphLaunch(e->gexec, e->stream), "graph launch");
         CK(cudaEventRecord(e->ev1, e->stream), "event");
+    } else if (o.mode == GEGS_MODE_TIMED) {
+        // Same kernels as the persistent graph, launched wave by wave with an
+        // event pair around each launch to attribute device time per kernel.
+        for (int k = 0; k < 12; k++) { e->last.stage_ms[k] = 0.0; e->last.stage_launches[k] = 0; }
+        std::vector<cudaEvent_t> evs(26);
+        for (auto &ev : evs) CK(cudaEventCreate(&ev), "event");
+        CK(cudaEventRecord(e->ev0, e->stream), "event");
+        SchedState hsr;
+        float acc[12] = {0};
+        unsigned long long nl[12] = {0};
+        for (uint32_t w = 0; w < max_waves; w++) {
+            CK(cudaEventRecord(evs[24], e->stream), "event");
+            k_plan<<<1, 1, 0, e->stream>>>(e->ctx, e->d_sched);
+            CK(cudaEventRecord(evs[25], e->stream), "event");
+            CK(cudaMemcpyAsync(&hsr, e->d_sched, sizeof hsr, cudaMemcpyDeviceToHost, e->stream), "sched D2H");
+            CK(cudaStreamSynchronize(e->stream), "timed sync");
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, evs[24], evs[25]);
+            acc[11] += t; nl[11]++;
+            if (!hsr.pending) break;
+            const DevCtx &C = e->ctx;
+            cudaStream_t s = e->stream;
+            int slot[11] = {10, ST_PHOTON, ST_COMPTON, ST_PHOTO, ST_RAYLEIGH, ST_PAIR, ST_ELECTRON, ST_MOLLER, ST_BREMS, ST_BHABHA, ST_ANNIH};
+            for (int k = 0; k < 11; k++) {
+                CK(cudaEventRecord(evs[2 * k], s), "event");
+                switch (slot[k]) {
+                case 10: k_source<<<grid, threads, 0, s>>>(C, e->d_sched); break;
+                case ST_PHOTON: k_photon<<<grid, threads, 0, s>>>(C); break;
+                case ST_COMPTON: k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(C); break;
+                case ST_PHOTO: k_interact<ST_PHOTO><<<grid, threads, 0, s>>>(C); break;
+                case ST_RAYLEIGH: k_interact<ST_RAYLEIGH><<<grid, threads, 0, s>>>(C); break;
+                case ST_PAIR: k_interact<ST_PAIR><<<grid, threads, 0, s>>>(C); break;
+                case ST_ELECTRON: k_electron<<<grid, threads, 0, s>>>(C); break;
+                case ST_MOLLER: k_interact<ST_MOLLER><<<grid, threads, 0, s>>>(C); break;
+                case ST_BREMS: k_interact<ST_BREMS><<<grid, threads, 0, s>>>(C); break;
+                case ST_BHABHA: k_interact<ST_BHABHA><<<grid, threads, 0, s>>>(C); break;
+                default: k_interact<ST_ANNIH><<<grid, threads, 0, s>>>(C); break;
+                }
+                CK(cudaEventRecord(evs[2 * k + 1], s), "event");
+            }
+            CK(cudaStreamSynchronize(s), "timed sync");
+            for (int k = 0; k < 11; k++) {
+                float tk = 0.0f;
+                cudaEventElapsedTime(&tk, evs[2 * k], evs[2 * k + 1]);
+                acc[slot[k]] += tk;
+                nl[slot[k]]++;
+            }
+        }
+        CK(cudaEventRecord(e->ev1, e->stream), "event");
+        for (auto &ev : evs) cudaEventDestroy(ev);
+        for (int k = 0; k < 12; k++) { e->last.stage_ms[k] = acc[k]; e->last.stage_launches[k] = nl[k]; }
     } else {
         // Plain form: host-driven, one kernel per event type, synchronise and
         // read the queue counters back after every launch (CUDA_EGS.cu:226-365).
         CK(cudaEventRecord(e->ev0, e->stream), "event");
-        uint32_t counts[GX_NSTAGE];
+        uint32_t counts[GX_NQ];
         SchedState hsr;
         for (uint32_t w = 0; w < max_waves; w++) {
             k_plan<<<1, 1, 0, e->stream>>>(e->ctx, e->d_sched);

@@ -24,7 +24,7 @@ struct SchedState {
     uint32_t batch, waves, max_waves, pending;
 };
 
-__device__ __forceinline__ void consumer_done(const DevCtx &C, int q)
+__device__ __forceinline__ void consumer_done(const DevCtx &C, int q, int q2 = -1)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -34,9 +34,46 @@ __device__ __forceinline__ void consumer_done(const DevCtx &C, int q)
             C.q.count[q] = 0;
             C.q.head[q] = 0;
             C.q.done[q] = 0;
+            if (q2 >= 0) C.q.count[q2] = 0;
             __threadfence();
         }
     }
+}
+
+// Re-queue a particle whose per-launch step budget ran out (same stream, same
+// state: the result does not depend on where a track is split).
+__device__ __forceinline__ void push_cont(const DevCtx &C, int qid, Part p, const Rng &r, const EStatePk *st)
+{
+    rng_store(r, p);
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(&C.q.count[qid], (uint32_t)g.size());
+    base = g.shfl(base, 0);
+    uint32_t idx = base + g.thread_rank();
+    if (idx < C.q.cap[qid]) {
+        store_part(&C.q.buf[qid][idx], p);
+        if (st) C.q.estate[(qid - GX_Q_ECONT) & 1][idx] = *st;
+    } else {
+        atomicOr(C.err, GX_ERR_QUEUE_FULL);
+    }
+}
+
+__device__ __forceinline__ EStatePk pack_estate(const EState &s)
+{
+    EStatePk k;
+    k.elke = s.elke; k.demfp = s.demfp; k.sig0 = s.sig0; k.total_tstep = s.total_tstep;
+    k.lelke = s.lelke;
+    k.flags = (s.compute_tstep ? 1u : 0u) | (s.is_tstep ? 2u : 0u);
+    k.pad0 = 0; k.pad1 = 0;
+    return k;
+}
+
+__device__ __forceinline__ void unpack_estate(const EStatePk &k, EState &s)
+{
+    s.elke = k.elke; s.demfp = k.demfp; s.sig0 = k.sig0; s.total_tstep = k.total_tstep;
+    s.lelke = k.lelke;
+    s.compute_tstep = (k.flags & 1u) != 0;
+    s.is_tstep = (k.flags & 2u) != 0;
 }
 
 __device__ __forceinline__ uint32_t queue_len(const DevCtx &C, int q)
@@ -104,8 +141,12 @@ __global__ void k_source(const __grid_constant__ DevCtx C, const SchedState *st)
 }
 
 // ---- persistent consumers with warp regeneration ---------------------------
-template <int Q>
-__device__ __forceinline__ bool refill(const DevCtx &C, uint32_t n, bool &exhausted, bool active, Part &p, Rng &r)
+// A consumer drains the continuation queue of the previous wave (indices
+// [0, n_cont)) and then its stage queue ([n_cont, n_cont + n_fresh)) through one
+// shared head counter; idle lanes of a warp are refilled with one atomic.
+template <int Q, bool ELEC>
+__device__ __forceinline__ bool refill(const DevCtx &C, uint32_t n_cont, uint32_t n, int qc, bool &exhausted,
+                                       bool active, Part &p, Rng &r, EState *s, unsigned long long &taken)
 {
     const uint32_t lane = threadIdx.x & 31u;
     unsigned need = __ballot_sync(0xffffffffu, !active);
@@ -118,9 +159,17 @@ __device__ __forceinline__ bool refill(const DevCtx &C, uint32_t n, bool &exhaus
     if (!active) {
         uint32_t idx = base + __popc(need & ((1u << lane) - 1u));
         if (idx < n) {
-            p = load_part(&C.q.buf[Q][idx]);
-            rng_load(r, p);
-            trace_event(C, 1u, Q, p);
+            if (idx < n_cont) {
+                p = load_part(&C.q.buf[qc][idx]);
+                rng_load(r, p);
+                if (ELEC) unpack_estate(C.q.estate[(qc - GX_Q_ECONT) & 1][idx], *s);
+            } else {
+                p = load_part(&C.q.buf[Q][idx - n_cont]);
+                rng_load(r, p);
+                if (ELEC) estate_init(*s);
+                trace_event(C, 1u, Q, p);
+                taken++;
+            }
             return true;
         }
     }
@@ -129,7 +178,10 @@ __device__ __forceinline__ bool refill(const DevCtx &C, uint32_t n, bool &exhaus
 
 __global__ void __launch_bounds__(256) k_photon(const __grid_constant__ DevCtx C)
 {
-    const uint32_t n = queue_len(C, ST_PHOTON);
+    const uint32_t par = *C.wave & 1u;
+    const int qc_in = GX_Q_PCONT + (int)par, qc_out = GX_Q_PCONT + (int)(par ^ 1u);
+    const uint32_t n_cont = queue_len(C, qc_in);
+    const uint32_t n = n_cont + queue_len(C, ST_PHOTON);
     Part p;
     Rng r;
     bool active = false, exhausted = false;
@@ -137,23 +189,26 @@ __global__ void __launch_bounds__(256) k_photon(const __grid_constant__ DevCtx C
     uint32_t nst = 0;
     for (;;) {
         bool was = active;
-        active = refill<ST_PHOTON>(C, n, exhausted, active, p, r);
-        if (active && !was) { taken++; nst = 0; }
+        active = refill<ST_PHOTON, false>(C, n_cont, n, qc_in, exhausted, active, p, r, nullptr, taken);
+        if (active && !was) nst = 0;
         if (!__any_sync(0xffffffffu, active)) break;
         if (active) {
             steps++;
             if (photon_step(C, p, r)) active = false;
-            else if (++nst > GX_STEP_BUDGET) { active = false; atomicOr(C.err, GX_ERR_STEP_BUDGET); }
+            else if (++nst >= C.photon_budget) { push_cont(C, qc_out, p, r, nullptr); active = false; }
         }
     }
     block_stat_add(C, ST_PHOTON, taken);
     block_stat_add(C, GX_NSTAGE, steps);
-    consumer_done(C, ST_PHOTON);
+    consumer_done(C, ST_PHOTON, qc_in);
 }
 
 __global__ void __launch_bounds__(256) k_electron(const __grid_constant__ DevCtx C)
 {
-    const uint32_t n = queue_len(C, ST_ELECTRON);
+    const uint32_t par = *C.wave & 1u;
+    const int qc_in = GX_Q_ECONT + (int)par, qc_out = GX_Q_ECONT + (int)(par ^ 1u);
+    const uint32_t n_cont = queue_len(C, qc_in);
+    const uint32_t n = n_cont + queue_len(C, ST_ELECTRON);
     Part p;
     Rng r;
     EState s;
@@ -162,18 +217,22 @@ __global__ void __launch_bounds__(256) k_electron(const __grid_constant__ DevCtx
     uint32_t nst = 0;
     for (;;) {
         bool was = active;
-        active = refill<ST_ELECTRON>(C, n, exhausted, active, p, r);
-        if (active && !was) { taken++; estate_init(s); nst = 0; }
+        active = refill<ST_ELECTRON, true>(C, n_cont, n, qc_in, exhausted, active, p, r, &s, taken);
+        if (active && !was) nst = 0;
         if (!__any_sync(0xffffffffu, active)) break;
         if (active) {
             steps++;
             if (electron_step(C, p, r, s)) active = false;
-            else if (++nst > GX_STEP_BUDGET) { active = false; atomicOr(C.err, GX_ERR_STEP_BUDGET); }
+            else if (++nst >= C.electron_budget) {
+                EStatePk k = pack_estate(s);
+                push_cont(C, qc_out, p, r, &k);
+                active = false;
+            }
         }
     }
     block_stat_add(C, ST_ELECTRON, taken);
     block_stat_add(C, GX_NSTAGE + 1, steps);
-    consumer_done(C, ST_ELECTRON);
+    consumer_done(C, ST_ELECTRON, qc_in);
 }
 
 template <int Q>
@@ -250,8 +309,9 @@ __global__ void __launch_bounds__(256) k_plain(const __grid_constant__ DevCtx C)
 __device__ __forceinline__ uint32_t plan_wave(const DevCtx &C, SchedState *st)
 {
     uint32_t inflight = 0;
-    for (int q = 0; q < GX_NSTAGE; q++) inflight += *((volatile uint32_t *)&C.q.count[q]);
+    for (int q = 0; q < GX_NQ; q++) inflight += *((volatile uint32_t *)&C.q.count[q]);
     uint32_t main_q = *((volatile uint32_t *)&C.q.count[ST_PHOTON]) + *((volatile uint32_t *)&C.q.count[ST_ELECTRON]);
+    for (int q = GX_Q_PCONT; q < GX_NQ; q++) main_q += *((volatile uint32_t *)&C.q.count[q]);
     unsigned long long remaining = st->end - st->next;
     unsigned long long inject = 0;
     if (remaining > 0 && main_q < st->batch / 2) inject = remaining < st->batch ? remaining : st->batch;

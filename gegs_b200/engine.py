@@ -16,7 +16,7 @@ LIB_PATH = pathlib.Path(__file__).resolve().parent / "libgegs_b200.so"
 
 STATUS = {0: "GEGS_OK", 1: "GEGS_ERR_ARG", 2: "GEGS_ERR_CUDA", 3: "GEGS_ERR_QUEUE_FULL", 4: "GEGS_ERR_MODULE",
           5: "GEGS_ERR_NOMEM", 6: "GEGS_ERR_STEP_BUDGET", 7: "GEGS_ERR_SOURCE"}
-MODE_PERSISTENT, MODE_PLAIN = 0, 1
+MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 
 EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
            "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_get_dose", "gegs_get_stats",
@@ -35,12 +35,13 @@ class GegsError(RuntimeError):
 
 class RunOpts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("batch", C.c_uint32), ("blocks_per_sm", C.c_int32),
-                ("threads_per_block", C.c_int32), ("max_waves", C.c_uint32), ("reserved", C.c_uint32)]
+                ("threads_per_block", C.c_int32), ("max_waves", C.c_uint32), ("step_budget", C.c_uint32)]
 
 
 class RunStats(C.Structure):
     _fields_ = [("processed", C.c_uint64 * 10), ("photon_steps", C.c_uint64), ("electron_steps", C.c_uint64),
-                ("waves", C.c_uint32), ("error_bits", C.c_uint32), ("device_ms", C.c_double)]
+                ("waves", C.c_uint32), ("error_bits", C.c_uint32), ("device_ms", C.c_double),
+                ("stage_ms", C.c_double * 12), ("stage_launches", C.c_uint64 * 12)]
 
 
 _lib = None
@@ -123,8 +124,8 @@ class Engine:
         self._check(self.L.gegs_set_phsp(self.h, r.ctypes.data, len(r)))
 
     def run(self, h0: int, h1: int, mode: int = MODE_PERSISTENT, batch: int = 0, blocks_per_sm: int = 0,
-            threads: int = 0, max_waves: int = 0):
-        o = RunOpts(mode, batch, blocks_per_sm, threads, max_waves, 0)
+            threads: int = 0, max_waves: int = 0, photon_budget: int = 0, electron_budget: int = 0):
+        o = RunOpts(mode, batch, blocks_per_sm, threads, max_waves, (photon_budget & 0xFFFF) | (electron_budget << 16))
         self._check(self.L.gegs_run(self.h, h0, h1, C.byref(o)))
         return self.stats()
 
@@ -146,7 +147,8 @@ class Engine:
         s = RunStats()
         self._check(self.L.gegs_get_stats(self.h, C.byref(s)))
         return dict(processed=list(s.processed), photon_steps=s.photon_steps, electron_steps=s.electron_steps,
-                    waves=s.waves, error_bits=s.error_bits, device_ms=s.device_ms)
+                    waves=s.waves, error_bits=s.error_bits, device_ms=s.device_ms,
+                    stage_ms=list(s.stage_ms), stage_launches=list(s.stage_launches))
 
     def set_trace(self, capacity: int):
         self._check(self.L.gegs_set_trace(self.h, capacity))

@@ -47,7 +47,9 @@ typedef enum gegs_status {
 
 typedef enum gegs_mode {
     GEGS_MODE_PERSISTENT = 0,  /* device-driven wave loop in one CUDA graph */
-    GEGS_MODE_PLAIN = 1        /* host loop: one kernel per event type, sync + counter read-back each launch */
+    GEGS_MODE_PLAIN = 1,       /* host loop: one kernel per event type, sync + counter read-back each launch */
+    GEGS_MODE_TIMED = 2        /* persistent kernels driven wave by wave from the host with CUDA events
+                                  around every launch (per-kernel device times in gegs_run_stats) */
 } gegs_mode;
 
 typedef struct gegs_run_opts {
@@ -56,7 +58,8 @@ typedef struct gegs_run_opts {
     int32_t blocks_per_sm;     /* 0 = default */
     int32_t threads_per_block; /* 0 = default */
     uint32_t max_waves;        /* safety budget (0 = default) */
-    uint32_t reserved;
+    uint32_t step_budget;      /* steps per particle per launch before it is continued in the next wave:
+                                  bits 0-15 photons, 16-31 electrons (0 = defaults 32 / 16) */
 } gegs_run_opts;
 
 typedef struct gegs_run_stats {
@@ -66,6 +69,8 @@ typedef struct gegs_run_stats {
     uint32_t waves;
     uint32_t error_bits;
     double device_ms;          /* device time of the last gegs_run (CUDA events) */
+    double stage_ms[12];       /* GEGS_MODE_TIMED: device ms per kernel kind (10 stages, source, planner) */
+    uint64_t stage_launches[12];
 } gegs_run_stats;
 
 /* Engine life cycle */

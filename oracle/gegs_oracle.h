@@ -13,6 +13,7 @@ typedef struct ora_stats {
     double e_escaped;             /* energy scored to regions 0..5 (not tallied) */
     int32_t error;
     int32_t pad_;
+    uint64_t cnt[10][3];   /* per stage: region records read, tally updates, float2 table reads */
 } ora_stats;
 
 size_t ora_sizeof_physics(void);

@@ -149,6 +149,7 @@ void gx_sincos(float a, float *s, float *c)
 void ora_escore(ora_ctx *C, uint32_t region, float energy)
 {
     if (region < VAC_AND_OTH) { C->e_escaped += (double)energy; return; }
+    C->cnt[C->cur_stage][1]++;
     C->tally[region - VAC_AND_OTH] += (int64_t)llrintf(energy * 1073741824.0f);
 }
 

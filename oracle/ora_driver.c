@@ -91,6 +91,7 @@ static int make_primary(const gegs_scene *S, uint64_t h, ora_particle *p)
 static void run_particle(ora_ctx *C, ora_particle *p)
 {
     C->counts[p->status]++;
+    C->cur_stage = p->status;
     ora_trace(C, 1u, p->status, p);
     switch (p->status) {
     case p_photon_step: ora_photon(C, p); break;
@@ -162,6 +163,8 @@ int ora_run(const gegs_physics *P, const gegs_scene *S, uint64_t h0, uint64_t h1
             tot.steps_photon += C.steps_photon;
             tot.steps_electron += C.steps_electron;
             tot.e_escaped += C.e_escaped;
+            for (int i = 0; i < ORA_NSTAGE; i++)
+                for (int k = 0; k < 3; k++) tot.cnt[i][k] += C.cnt[i][k];
             err |= C.error;
             if (g_trace) g_trace_n = C.trace_n;
         }

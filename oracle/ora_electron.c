@@ -18,7 +18,8 @@
 
 static inline float U(ora_ctx *C, ora_rng *r) { return ora_rng_uniform(C, r); }
 
-static inline float ev2(const float *t, float x) { return t[0] + t[1] * x; }
+static _Thread_local uint64_t *g_table_counter;   /* electron-stage table-read counter of the running thread */
+static inline float ev2(const float *t, float x) { if (g_table_counter) (*g_table_counter)++; return t[0] + t[1] * x; }
 
 static void box_phi(ora_ctx *C, ora_rng *r, float *cphi, float *sphi)
 {
@@ -203,6 +204,7 @@ static void msdist_pI(ora_ctx *C, float eloss, float tustep, ora_particle *p0, f
 static float range_piece(const gegs_physics *P, int qel, unsigned medium, int lel, float elk_a, float elk_b, float e_hi, float fedep)
 {
     float elktmp = 0.5f * (elk_a + elk_b + 0.25f * fedep * fedep * (1.0f + fedep * (1.0f + 0.875f * fedep)));
+    if (g_table_counter) (*g_table_counter)++;
     const float *d = P->dedx[qel * MXEKE * MXMED + medium * MXEKE + lel - 1];
     float dedxmid = d[0] + d[1] * elktmp;
     dedxmid = 1.0f / dedxmid;
@@ -260,12 +262,14 @@ static void e_discard_below_cut(ora_ctx *C, ora_particle *p, const ora_region *r
 
 void ora_electron(ora_ctx *C, ora_particle *p)
 {
+    g_table_counter = &C->cnt[e_electron_step][2];
     const gegs_physics *P = C->P;
     const float rm = P->rm, prm = P->prm, rmt2 = P->rmt2, rmsq = P->rmsq;
     float elke = 0.0f, demfp = 0.0f, sig0 = 0.0f, total_tstep = 0.0f;
     int lelke = 0, compute_tstep = 1, is_tstep = 1;
     for (;;) {
         C->steps_electron++;
+        C->cnt[e_electron_step][0]++;
         uint32_t irold = p->region, irl = irold;
         const ora_region *rd = &C->reg[irl];
         unsigned medium = rd->med;
@@ -491,6 +495,7 @@ void ora_electron(ora_ctx *C, ora_particle *p)
             irl = irnew;
             rd = &C->reg[irl];
             medium = rd->med;
+            C->cnt[e_electron_step][0]++;
         }
         if (eie <= rd->ecut) { e_discard_below_cut(C, p, rd); return; }
         if (idisc < 0) {

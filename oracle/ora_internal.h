@@ -120,6 +120,10 @@ typedef struct {
     uint64_t steps_photon, steps_electron;
     double e_escaped;        /* energy leaving through region 0 (for conservation audits) */
     int error;
+    /* algorithmic-traffic counters per stage: [0] region records read,
+     * [1] tally updates, [2] float2 table reads */
+    uint64_t cnt[ORA_NSTAGE][3];
+    int cur_stage;
     ora_trace_rec *trace;    /* debug trace (single-threaded runs only) */
     uint32_t trace_n, trace_cap;
 } ora_ctx;

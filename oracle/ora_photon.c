@@ -59,6 +59,7 @@ void ora_photon(ora_ctx *C, ora_particle *p)
     const float rm2 = 2.0f * P->rm;
     for (;;) {
         C->steps_photon++;
+        C->cnt[p_photon_step][0]++;
         const ora_region *rd = &C->reg[p->region];
         if (p->e <= rd->pcut) { ora_escore(C, p->region, p->e * p->wt); return; }
         if (p->wt <= 0.0f) return;
@@ -71,6 +72,7 @@ void ora_photon(ora_ctx *C, ora_particle *p)
         if (med == VACUUM) tstep = VACUUM_STEP;
         else {
             lgle = (int)(P->ge[med][0] + P->ge[med][1] * gle);
+            C->cnt[p_photon_step][2] += 2 + ((rd->flags & GEGS_F_RAYLEIGH) ? 1 : 0);
             const float *g = P->gmfp[med * MXGE + lgle];
             float gmfpr0 = g[0] + g[1] * gle;
             gmfp_val = gmfpr0 / rd->rhof;
@@ -94,13 +96,14 @@ void ora_photon(ora_ctx *C, ora_particle *p)
         p->z = p->z + p->w * tstep;
         if (med != VACUUM) dpmfp = fmaxf_(0.0f, dpmfp - tstep / gmfp_val);
         unsigned old_medium = med;
-        if (new_region != p->region) { p->region = new_region; rd = &C->reg[new_region]; }
+        if (new_region != p->region) { p->region = new_region; rd = &C->reg[new_region]; C->cnt[p_photon_step][0]++; }
         if (p->e <= rd->pcut || idisc < 0) { ora_escore(C, p->region, p->e * p->wt); return; }
         if ((rd->med != old_medium) || (rd->med == VACUUM) || (dpmfp >= EPSGMFP)) continue;
         if (rd->flags & GEGS_F_RAYLEIGH) {
             r1 = U(C, &p->rng);
             if (r1 < 1.0f - cohfac) { ora_push(C, p, p_rayleigh); return; }
         }
+        C->cnt[p_photon_step][2] += 2;
         const float *b1 = P->gbr1[rd->med * MXGE + lgle];
         const float *b2 = P->gbr2[rd->med * MXGE + lgle];
         float gbr1_val = b1[0] + b1[1] * gle;

@@ -19,7 +19,8 @@ LIB = HERE / "_build" / "libgegs_oracle.so"
 
 class Stats(C.Structure):
     _fields_ = [("counts", C.c_uint64 * 10), ("steps_photon", C.c_uint64), ("steps_electron", C.c_uint64),
-                ("e_escaped", C.c_double), ("error", C.c_int32), ("pad_", C.c_int32)]
+                ("e_escaped", C.c_double), ("error", C.c_int32), ("pad_", C.c_int32),
+                ("cnt", (C.c_uint64 * 3) * 10)]
 
 
 def build(force=False):
@@ -83,5 +84,6 @@ def run(physics: np.ndarray, scene_holder, h0: int, h1: int, threads: int = 0):
     rc = L.ora_run(phys.ctypes.data, C.addressof(scene_holder.scene), h0, h1, threads or os.cpu_count(),
                    tally.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(st))
     stats = dict(counts=list(st.counts), steps_photon=st.steps_photon, steps_electron=st.steps_electron,
-                 e_escaped=st.e_escaped, error=st.error, rc=rc)
+                 e_escaped=st.e_escaped, error=st.error, rc=rc,
+                 cnt=[list(st.cnt[i]) for i in range(10)])
     return tally, stats

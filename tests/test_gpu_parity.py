@@ -89,3 +89,29 @@ def test_run_to_run_identical(engine):
     a, _, _ = _run(engine, job, 0, job.histories)
     b, _, _ = _run(engine, job, 0, job.histories)
     _assert_same(a, b)
+
+
+def test_step_budget_does_not_change_result(engine, oracle):
+    """Tracks split across launches (continuation queues) give the same tally
+    as tracks run to the end in one launch, and as the oracle."""
+    job = W.config3(histories=6000, nphsp=5000, dims=(48, 48, 24))
+    a, sa, sh = _run(engine, job, 0, job.histories, photon_budget=1, electron_budget=1)
+    b, sb, _ = _run(engine, job, 0, job.histories, photon_budget=8, electron_budget=3)
+    c, sc, _ = _run(engine, job, 0, job.histories, photon_budget=60000, electron_budget=60000)
+    ref, rst = oracle.run(job.physics, sh, 0, job.histories)
+    _assert_same(a, ref)
+    _assert_same(b, ref)
+    _assert_same(c, ref)
+    assert sa["processed"] == sc["processed"]
+    assert sa["electron_steps"] == sc["electron_steps"] and sa["photon_steps"] == sc["photon_steps"]
+    assert sa["waves"] > sc["waves"]
+
+
+def test_timed_mode_bit_exact(engine, oracle):
+    from gegs_b200.engine import MODE_TIMED
+    job = W.config2(histories=4000, nphsp=4000, n=30)
+    gpu, st, sh = _run(engine, job, 0, job.histories, mode=MODE_TIMED)
+    ref, _ = oracle.run(job.physics, sh, 0, job.histories)
+    _assert_same(gpu, ref)
+    assert st["stage_launches"][0] == st["waves"] - 1 or st["stage_launches"][0] >= 1
+    assert sum(st["stage_ms"]) > 0
