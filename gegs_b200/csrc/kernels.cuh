@@ -22,6 +22,7 @@ struct SchedState {
     unsigned long long next, end;     // history cursor
     unsigned long long h0, h1;        // histories injected by the current wave
     uint32_t batch, waves, max_waves, pending;
+    uint32_t refill_below;
 };
 
 __device__ __forceinline__ void consumer_done(const DevCtx &C, int q, int q2 = -1)
@@ -176,7 +177,16 @@ __device__ __forceinline__ bool refill(const DevCtx &C, uint32_t n_cont, uint32_
     return active;
 }
 
-__global__ void __launch_bounds__(256) k_photon(const __grid_constant__ DevCtx C)
+// Register caps of the two transport consumers (minimum resident 256-thread
+// blocks per SM); measured best on the CT 5-field plan.
+#ifndef GX_PHOTON_MIN_BLOCKS
+#define GX_PHOTON_MIN_BLOCKS 4
+#endif
+#ifndef GX_ELECTRON_MIN_BLOCKS
+#define GX_ELECTRON_MIN_BLOCKS 3
+#endif
+
+__global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon(const __grid_constant__ DevCtx C)
 {
     const uint32_t par = *C.wave & 1u;
     const int qc_in = GX_Q_PCONT + (int)par, qc_out = GX_Q_PCONT + (int)(par ^ 1u);
@@ -203,7 +213,7 @@ __global__ void __launch_bounds__(256) k_photon(const __grid_constant__ DevCtx C
     consumer_done(C, ST_PHOTON, qc_in);
 }
 
-__global__ void __launch_bounds__(256) k_electron(const __grid_constant__ DevCtx C)
+__global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron(const __grid_constant__ DevCtx C)
 {
     const uint32_t par = *C.wave & 1u;
     const int qc_in = GX_Q_ECONT + (int)par, qc_out = GX_Q_ECONT + (int)(par ^ 1u);
@@ -312,9 +322,13 @@ __device__ __forceinline__ uint32_t plan_wave(const DevCtx &C, SchedState *st)
     for (int q = 0; q < GX_NQ; q++) inflight += *((volatile uint32_t *)&C.q.count[q]);
     uint32_t main_q = *((volatile uint32_t *)&C.q.count[ST_PHOTON]) + *((volatile uint32_t *)&C.q.count[ST_ELECTRON]);
     for (int q = GX_Q_PCONT; q < GX_NQ; q++) main_q += *((volatile uint32_t *)&C.q.count[q]);
+    // once the population falls below `refill_below`, top it up to `batch`
     unsigned long long remaining = st->end - st->next;
     unsigned long long inject = 0;
-    if (remaining > 0 && main_q < st->batch / 2) inject = remaining < st->batch ? remaining : st->batch;
+    if (remaining > 0 && main_q < st->refill_below && main_q < st->batch) {
+        inject = st->batch - main_q;
+        if (inject > remaining) inject = remaining;
+    }
     st->h0 = st->next;
     st->h1 = st->next + inject;
     st->next += inject;

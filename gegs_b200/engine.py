@@ -35,7 +35,8 @@ class GegsError(RuntimeError):
 
 class RunOpts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("batch", C.c_uint32), ("blocks_per_sm", C.c_int32),
-                ("threads_per_block", C.c_int32), ("max_waves", C.c_uint32), ("step_budget", C.c_uint32)]
+                ("threads_per_block", C.c_int32), ("max_waves", C.c_uint32), ("step_budget", C.c_uint32),
+                ("refill_below", C.c_uint32)]
 
 
 class RunStats(C.Structure):
@@ -124,8 +125,10 @@ class Engine:
         self._check(self.L.gegs_set_phsp(self.h, r.ctypes.data, len(r)))
 
     def run(self, h0: int, h1: int, mode: int = MODE_PERSISTENT, batch: int = 0, blocks_per_sm: int = 0,
-            threads: int = 0, max_waves: int = 0, photon_budget: int = 0, electron_budget: int = 0):
-        o = RunOpts(mode, batch, blocks_per_sm, threads, max_waves, (photon_budget & 0xFFFF) | (electron_budget << 16))
+            threads: int = 0, max_waves: int = 0, photon_budget: int = 0, electron_budget: int = 0,
+            refill_below: int = 0):
+        o = RunOpts(mode, batch, blocks_per_sm, threads, max_waves, (photon_budget & 0xFFFF) | (electron_budget << 16),
+                    refill_below)
         self._check(self.L.gegs_run(self.h, h0, h1, C.byref(o)))
         return self.stats()
 
