@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 #include "kernels.cuh"
@@ -535,5 +536,151 @@ extern "C" gegs_status gegs_tally_device_ptr(gegs_engine *e, void **out)
 {
     if (!e || !out || !e->d_tally) return GEGS_ERR_ARG;
     *out = e->d_tally;
+    return GEGS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// gegs_run_noalloc: the wave loop with every piece of scratch memory (queue
+// counters, scheduler state, error word, counters, the 14 event queues and the
+// electron continuation state) carved from one fixed device array, so that a
+// run allocates nothing.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t noalloc_align(size_t x) { return (x + 255u) & ~(size_t)255u; }
+
+// Upper bound of the carve-out at GEGS_NOALLOC_MAX_BATCH: the queue capacity
+// factors sum to 60, the electron continuation queues have factor 6, and
+// every queue has 4096 spare slots.
+constexpr size_t kNoallocBytes =
+    noalloc_align(sizeof(uint32_t) * 3 * GX_NQ) + noalloc_align(sizeof(SchedState)) +
+    noalloc_align(sizeof(uint32_t)) + noalloc_align(sizeof(unsigned long long) * 16) +
+    (60ull * GEGS_NOALLOC_MAX_BATCH + (size_t)GX_NQ * 4096u) * sizeof(Part) + (size_t)GX_NQ * 256u +
+    2u * (noalloc_align((6ull * GEGS_NOALLOC_MAX_BATCH + 4096u) * sizeof(EStatePk)));
+
+constexpr int kNoallocMaxDevices = 64;
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+static std::mutex g_noalloc_mu;
+static unsigned char *g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `device` (the current device); looked
+// up once per device. Host code must not use the symbol itself as a pointer.
+static cudaError_t noalloc_scratch(int device, unsigned char **out)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void *p = nullptr;
+        cudaError_t c = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (c != cudaSuccess) return c;
+        g_noalloc_ptr[device] = (unsigned char *)p;
+    }
+    *out = g_noalloc_ptr[device];
+    return cudaSuccess;
+}
+
+extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, uint32_t batch)
+{
+    if (!e) return GEGS_ERR_ARG;
+    if (!e->have_scene || hist_end < hist_begin) { e->err = "gegs_run_noalloc: no scene, or hist_end < hist_begin"; return GEGS_ERR_ARG; }
+    if (batch == 0) batch = GEGS_NOALLOC_MAX_BATCH;
+    if (batch > GEGS_NOALLOC_MAX_BATCH) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "gegs_run_noalloc: batch %u exceeds the fixed scratch limit of %u particles "
+                 "(GEGS_NOALLOC_MAX_BATCH)", batch, GEGS_NOALLOC_MAX_BATCH);
+        e->err = buf;
+        return GEGS_ERR_ARG;
+    }
+    if (e->device < 0 || e->device >= kNoallocMaxDevices) { e->err = "gegs_run_noalloc: device index out of range"; return GEGS_ERR_ARG; }
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    unsigned char *base = nullptr;
+    CK(noalloc_scratch(e->device, &base), "gegs_run_noalloc: cudaGetSymbolAddress of the scratch array");
+
+    // carve the array
+    size_t off = 0;
+    auto take = [&](size_t bytes) { unsigned char *p = base + off; off += noalloc_align(bytes); return p; };
+    uint32_t *qmeta = (uint32_t *)take(sizeof(uint32_t) * 3 * GX_NQ);
+    SchedState *sched = (SchedState *)take(sizeof(SchedState));
+    uint32_t *err = (uint32_t *)take(sizeof(uint32_t));
+    unsigned long long *stats = (unsigned long long *)take(sizeof(unsigned long long) * 16);
+    const size_t zero_bytes = off;   // counters, scheduler, error word and stats start at zero
+    DevCtx c = e->ctx;
+    for (int q = 0; q < GX_NQ; q++) {
+        uint32_t cap = (uint32_t)(kCapFactor[q] * (float)batch) + 4096u;
+        c.q.cap[q] = cap;
+        c.q.buf[q] = (Part *)take((size_t)cap * sizeof(Part));
+    }
+    for (int k = 0; k < 2; k++) c.q.estate[k] = (EStatePk *)take((size_t)c.q.cap[GX_Q_ECONT + k] * sizeof(EStatePk));
+    if (off > kNoallocBytes) { e->err = "gegs_run_noalloc: scratch layout exceeds the array"; return GEGS_ERR_ARG; }
+    c.q.count = qmeta;
+    c.q.head = qmeta + GX_NQ;
+    c.q.done = qmeta + 2 * GX_NQ;
+    c.err = err;
+    c.stats = stats;
+    c.wave = &sched->waves;
+    c.trace = nullptr;
+    c.trace_n = nullptr;
+    c.trace_cap = 0;
+    c.photon_budget = 16u;
+    c.electron_budget = 8u;
+
+    SchedState hs = {};
+    hs.next = hist_begin;
+    hs.end = hist_end;
+    hs.batch = batch;
+    hs.max_waves = 200000u;
+    hs.refill_below = batch / 50u > 0u ? batch / 50u : 1u;
+    cudaStream_t s = e->stream;
+    CK(cudaMemsetAsync(base, 0, zero_bytes, s), "gegs_run_noalloc: scratch reset");
+    CK(cudaMemcpyAsync(sched, &hs, sizeof hs, cudaMemcpyHostToDevice, s), "gegs_run_noalloc: scheduler H2D");
+
+    const int threads = 256, grid = e->nsm * 4;
+    CK(cudaEventRecord(e->ev0, s), "event");
+    SchedState hsr = {};
+    for (uint32_t w = 0; w < hs.max_waves;) {
+        // a few waves between host checks; waves after the last one find empty queues
+        for (int k = 0; k < 8 && w < hs.max_waves; k++, w++) {
+            k_plan<<<1, 1, 0, s>>>(c, sched);
+            k_source<<<grid, threads, 0, s>>>(c, sched);
+            k_photon<<<grid, threads, 0, s>>>(c);
+            k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(c);
+            k_interact<ST_PHOTO><<<grid, threads, 0, s>>>(c);
+            k_interact<ST_RAYLEIGH><<<grid, threads, 0, s>>>(c);
+            k_interact<ST_PAIR><<<grid, threads, 0, s>>>(c);
+            k_electron<<<grid, threads, 0, s>>>(c);
+            k_interact<ST_MOLLER><<<grid, threads, 0, s>>>(c);
+            k_interact<ST_BREMS><<<grid, threads, 0, s>>>(c);
+            k_interact<ST_BHABHA><<<grid, threads, 0, s>>>(c);
+            k_interact<ST_ANNIH><<<grid, threads, 0, s>>>(c);
+        }
+        CK(cudaGetLastError(), "gegs_run_noalloc: launch");
+        CK(cudaMemcpyAsync(&hsr, sched, sizeof hsr, cudaMemcpyDeviceToHost, s), "gegs_run_noalloc: scheduler D2H");
+        CK(cudaStreamSynchronize(s), "gegs_run_noalloc: sync");
+        if (!hsr.pending) break;
+    }
+    CK(cudaEventRecord(e->ev1, s), "event");
+    uint32_t errbits = 0;
+    unsigned long long st[16];
+    CK(cudaMemcpyAsync(&errbits, err, sizeof errbits, cudaMemcpyDeviceToHost, s), "gegs_run_noalloc: err D2H");
+    CK(cudaMemcpyAsync(st, stats, sizeof st, cudaMemcpyDeviceToHost, s), "gegs_run_noalloc: stats D2H");
+    CK(cudaStreamSynchronize(s), "gegs_run_noalloc: sync");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    gegs_run_stats &R = e->last;
+    R = gegs_run_stats{};
+    for (int q = 0; q < GX_NSTAGE; q++) R.processed[q] = st[q];
+    R.photon_steps = st[GX_NSTAGE];
+    R.electron_steps = st[GX_NSTAGE + 1];
+    R.waves = hsr.waves;
+    R.error_bits = errbits;
+    R.device_ms = ms;
+    if (errbits & GX_ERR_QUEUE_FULL) { e->err = "event queue overflow"; return GEGS_ERR_QUEUE_FULL; }
+    if (errbits & GX_ERR_MODULE) { e->err = "particle in an unsupported module"; return GEGS_ERR_MODULE; }
+    if (errbits & GX_ERR_SOURCE) { e->err = "history outside every field range"; return GEGS_ERR_SOURCE; }
+    if (errbits & GX_ERR_STEP_BUDGET) { e->err = "wave budget exhausted"; return GEGS_ERR_STEP_BUDGET; }
+    if (hsr.pending) { e->err = "wave budget exhausted"; return GEGS_ERR_STEP_BUDGET; }
     return GEGS_OK;
 }

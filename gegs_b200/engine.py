@@ -20,7 +20,7 @@ MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 
 EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
            "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_get_dose", "gegs_get_stats",
-           "gegs_tally_device_ptr", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version"]
+           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version"]
 
 
 TRACE_DTYPE = np.dtype([("kind_stage", "<u4"), ("hist_lo", "<u4"), ("sid_lo", "<u4"), ("sid_hi", "<u4"),
@@ -64,6 +64,7 @@ def load_library(path=None):
     L.gegs_set_scene.argtypes = [vp, vp]
     L.gegs_set_phsp.argtypes = [vp, vp, C.c_uint64]
     L.gegs_run.argtypes = [vp, C.c_uint64, C.c_uint64, C.POINTER(RunOpts)]
+    L.gegs_run_noalloc.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint32]
     L.gegs_reset_tally.argtypes = [vp]
     L.gegs_get_tally.argtypes = [vp, vp, C.c_uint64]
     L.gegs_get_dose.argtypes = [vp, vp, C.c_double, vp, C.c_uint64]

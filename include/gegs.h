@@ -95,6 +95,33 @@ gegs_status gegs_set_phsp(gegs_engine *e, const gegs_phsp_record *recs, uint64_t
  * the int64 tally (MeV * 2^30 per voxel).  opts may be NULL. */
 gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts);
 
+/* No counterpart in the reference: an addition of this library.
+ *
+ * gegs_run_noalloc transports histories [hist_begin, hist_end) like gegs_run
+ * and adds to the same tally, but it allocates no device memory. Its event
+ * queues, scheduler state and counters live in one fixed array compiled into
+ * the library (about 21 MB, held on every GPU that loads the library until the
+ * process exits). Use it when the caller cannot allocate at run time:
+ *   - a planning system or dose server that reserved the GPU's memory when it
+ *     started, where a later cudaMalloc of gegs_run's queues (several GB at
+ *     the default batch) fails or breaks up its pool;
+ *   - a latency-bound loop that cannot absorb cudaFree's device-wide
+ *     synchronisation.
+ * The scene, physics tables and tally are still the engine's, set up
+ * beforehand with gegs_create, gegs_set_physics and gegs_set_scene.
+ *
+ * batch = particles kept in flight: 0 means GEGS_NOALLOC_MAX_BATCH. Larger
+ * values return GEGS_ERR_ARG. A small batch transports far fewer histories per
+ * second than gegs_run with its default batch; the tally is the same bit for
+ * bit. The first call on a device looks up the array's device address and
+ * loads the library's kernels on that device, so make it before any stream
+ * capture on that device. Every call on a device shares the one array; the
+ * call clears the counters that must start at zero, but calls that overlap on
+ * the same GPU (two engines, two threads) race on it and must be serialised
+ * by the caller. The call returns when the transport is done. */
+#define GEGS_NOALLOC_MAX_BATCH 4096u
+gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, uint32_t batch);
+
 gegs_status gegs_reset_tally(gegs_engine *e);
 
 /* Copy the int64 tally (nvox entries) to host memory. */
