@@ -322,8 +322,10 @@ def main():
         crate, cn, cdt, cores = cpu_histories_per_s(job, seconds=args.cpu_seconds)
         cpu = {"value": crate, "unit": "histories/s", "cores": cores, "kind": "port",
                "sample": f"{cn} C3 histories in {cdt:.1f} s on {cores} host threads (CPU oracle, same inputs)"}
-    # per step: the first planner launch, then per wave the source, 10 stage kernels and the planner
-    launches_per_step = [1 + 12 * (st["waves"] - 1) for st in stats]
+    # per step: the first planner launch, then per wave the source, the stage kernels (the
+    # persistent form runs photon and electron transport as phantom + linac-head kernels) and the planner
+    per_wave = 12 if args.mode == "plain" else 14
+    launches_per_step = [1 + per_wave * (st["waves"] - 1) for st in stats]
     line = {
         "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed_s * 1e3 / args.steps, "higher_is_better": True,

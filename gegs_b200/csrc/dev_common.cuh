@@ -40,11 +40,15 @@ static_assert(sizeof(gegs_field) % 16 == 0, "field record size");
 #define GX_MXGE GEGS_MXGE
 #define GX_MXEKE GEGS_MXEKE
 #define GX_NSTAGE 10
-// queues: 10 event stages, then ping-pong continuation queues for photons
-// (10, 11) and electrons (12, 13) that a budget-limited consumer re-queues into
+// queues: 10 event stages, then ping-pong continuation queues that the
+// step-budgeted consumers re-queue into: photons in the phantom (10, 11) and in
+// the linac head (12, 13), electrons in the phantom (14, 15) and in the head
+// (16, 17). Electron continuations carry their step state (estate[qid - 14]).
 #define GX_Q_PCONT 10
-#define GX_Q_ECONT 12
-#define GX_NQ 14
+#define GX_Q_PHCONT 12
+#define GX_Q_ECONT 14
+#define GX_Q_EHCONT 16
+#define GX_NQ 18
 #define GX_LOOP_CAP 1000
 #define GX_EPSGMFP 1.e-5f
 #define GX_EPSEMFP 1.e-5f
@@ -104,7 +108,7 @@ struct __align__(16) EStatePk {
 struct QueueSet {
     Part *buf[GX_NQ];
     uint32_t cap[GX_NQ];
-    EStatePk *estate[2];  // state of the two electron continuation queues
+    EStatePk *estate[4];  // state of the four electron continuation queues
     uint32_t *count;      // [GX_NQ] items queued
     uint32_t *head;       // [GX_NQ] items taken by the running consumer
     uint32_t *done;       // [GX_NQ] finished blocks of the running consumer

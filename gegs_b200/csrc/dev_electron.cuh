@@ -244,6 +244,7 @@ __device__ __forceinline__ void e_discard_below_cut(const DevCtx &C, Part &p, co
 
 // One iteration of the ELECTR loop.  Returns true when the particle has left
 // the electron stage.
+template <int G = GX_GEOM_ALL>
 __device__ bool electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
 {
     const gegs_physics *P = C.P;
@@ -332,7 +333,7 @@ __device__ bool electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
         tmxs_val = fminf_(tmxs_val, P->smaxir[medium]);
         tustep = fminf_(tstep, fminf_(tmxs_val, range));
         bool ok;
-        hownear(C, p, tperp, ok);
+        hownear_g<G>(C, p, tperp, ok);
         if (!ok) { atomicOr(C.err, GX_ERR_MODULE); return true; }
         if (P->i_do_rr[medium] == 1 && p.e < P->e_max_rr[medium]) {
             if (tperp >= range) { e_discard_below_cut(C, p, rd, r); return true; }
@@ -381,7 +382,7 @@ __device__ bool electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
     float ustep0 = ustep;
     if (callhowfar || p.wt <= 0.0f) {
         bool ok;
-        irnew = howfar(C, p, ustep, ok);
+        irnew = howfar_g<G>(C, p, ustep, ok);
         if (!ok) { atomicOr(C.err, GX_ERR_MODULE); return true; }
     }
     if (irnew == 0) {

@@ -583,3 +583,57 @@ __device__ __forceinline__ void hownear(const DevCtx &C, Part &p, float &tperp, 
     default: ok = false; tperp = 0; return;
     }
 }
+
+// Geometry classes: a consumer kernel compiled for one class contains only that
+// class's geometry code (phantom voxels, or jaws + MLC of the linac head), which
+// keeps the code a divergent warp runs small. A particle whose module is outside
+// the class is handed to the other class's kernel between steps.
+#define GX_GEOM_ALL 0
+#define GX_GEOM_PHANTOM 1
+#define GX_GEOM_HEAD 2
+
+template <int G>
+__device__ __forceinline__ bool in_geom_class(const Part &p)
+{
+    if (G == GX_GEOM_PHANTOM) return p.module == GEGS_M_PHANTOM;
+    if (G == GX_GEOM_HEAD) return p.module != GEGS_M_PHANTOM;
+    return true;
+}
+
+template <int G>
+__device__ __forceinline__ uint32_t howfar_g(const DevCtx &C, Part &p, float &t, bool &ok)
+{
+    if (G == GX_GEOM_ALL) return howfar(C, p, t, ok);
+    ok = true;
+    if (G == GX_GEOM_PHANTOM) {
+        if (p.module == GEGS_M_PHANTOM) return howfar_phantom(C, p, t);
+    } else {
+        switch (p.module) {
+        case GEGS_M_VARMLC: return howfar_mlc(C, p, t);
+        case GEGS_M_SECJAWY: return howfar_secjaws_y(C, p, t);
+        case GEGS_M_SECJAWX: return howfar_secjaws_x(C, p, t);
+        default: break;
+        }
+    }
+    ok = false;
+    return 0;
+}
+
+template <int G>
+__device__ __forceinline__ void hownear_g(const DevCtx &C, Part &p, float &tperp, bool &ok)
+{
+    if (G == GX_GEOM_ALL) { hownear(C, p, tperp, ok); return; }
+    ok = true;
+    if (G == GX_GEOM_PHANTOM) {
+        if (p.module == GEGS_M_PHANTOM) { hownear_phantom(C, p, tperp); return; }
+    } else {
+        switch (p.module) {
+        case GEGS_M_VARMLC: hownear_mlc(C, p, tperp); return;
+        case GEGS_M_SECJAWY: hownear_secjaws_y(C, p, tperp); return;
+        case GEGS_M_SECJAWX: hownear_secjaws_x(C, p, tperp); return;
+        default: break;
+        }
+    }
+    ok = false;
+    tperp = 0;
+}

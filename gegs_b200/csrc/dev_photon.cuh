@@ -166,6 +166,7 @@ __device__ void relax(const DevCtx &C, float energy, int n, int iz, float &edep,
 
 // One iteration of the PHOTON loop.  Returns true when the photon has left
 // the photon stage (absorbed, escaped or queued for an interaction).
+template <int G = GX_GEOM_ALL>
 __device__ bool photon_step(const DevCtx &C, Part &p, Rng &r)
 {
     const gegs_physics *P = C.P;
@@ -193,7 +194,7 @@ __device__ bool photon_step(const DevCtx &C, Part &p, Rng &r)
         tstep = gmfp_val * dpmfp;
     }
     bool ok;
-    uint32_t new_region = howfar(C, p, tstep, ok);
+    uint32_t new_region = howfar_g<G>(C, p, tstep, ok);
     if (!ok) { atomicOr(C.err, GX_ERR_MODULE); return true; }
     int idisc = 0;
     if (new_region == 0) {

@@ -53,7 +53,7 @@ __device__ __forceinline__ void push_cont(const DevCtx &C, int qid, Part p, cons
     uint32_t idx = base + g.thread_rank();
     if (idx < C.q.cap[qid]) {
         store_part(&C.q.buf[qid][idx], p);
-        if (st) C.q.estate[(qid - GX_Q_ECONT) & 1][idx] = *st;
+        if (st) C.q.estate[qid - GX_Q_ECONT][idx] = *st;
     } else {
         atomicOr(C.err, GX_ERR_QUEUE_FULL);
     }
@@ -143,10 +143,10 @@ __global__ void k_source(const __grid_constant__ DevCtx C, const SchedState *st)
 
 // ---- persistent consumers with warp regeneration ---------------------------
 // A consumer drains the continuation queue of the previous wave (indices
-// [0, n_cont)) and then its stage queue ([n_cont, n_cont + n_fresh)) through one
-// shared head counter; idle lanes of a warp are refilled with one atomic.
+// [0, n_cont)) and then its stage queue ([n_cont, n)) through one shared head
+// counter `hq`; idle lanes of a warp are refilled with one atomic.
 template <int Q, bool ELEC>
-__device__ __forceinline__ bool refill(const DevCtx &C, uint32_t n_cont, uint32_t n, int qc, bool &exhausted,
+__device__ __forceinline__ bool refill(const DevCtx &C, int hq, uint32_t n_cont, uint32_t n, int qc, bool &exhausted,
                                        bool active, Part &p, Rng &r, EState *s, unsigned long long &taken)
 {
     const uint32_t lane = threadIdx.x & 31u;
@@ -154,7 +154,7 @@ __device__ __forceinline__ bool refill(const DevCtx &C, uint32_t n_cont, uint32_
     if (need == 0u || exhausted) return active;
     uint32_t cnt = __popc(need);
     uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&C.q.head[Q], cnt);
+    if (lane == 0) base = atomicAdd(&C.q.head[hq], cnt);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base + cnt >= n) exhausted = true;
     if (!active) {
@@ -163,7 +163,7 @@ __device__ __forceinline__ bool refill(const DevCtx &C, uint32_t n_cont, uint32_
             if (idx < n_cont) {
                 p = load_part(&C.q.buf[qc][idx]);
                 rng_load(r, p);
-                if (ELEC) unpack_estate(C.q.estate[(qc - GX_Q_ECONT) & 1][idx], *s);
+                if (ELEC) unpack_estate(C.q.estate[qc - GX_Q_ECONT][idx], *s);
             } else {
                 p = load_part(&C.q.buf[Q][idx - n_cont]);
                 rng_load(r, p);
@@ -177,7 +177,7 @@ __device__ __forceinline__ bool refill(const DevCtx &C, uint32_t n_cont, uint32_
     return active;
 }
 
-// Register caps of the two transport consumers (minimum resident 256-thread
+// Register caps of the transport consumers (minimum resident 256-thread
 // blocks per SM); measured best on the CT 5-field plan.
 #ifndef GX_PHOTON_MIN_BLOCKS
 #define GX_PHOTON_MIN_BLOCKS 4
@@ -186,39 +186,28 @@ __device__ __forceinline__ bool refill(const DevCtx &C, uint32_t n_cont, uint32_
 #define GX_ELECTRON_MIN_BLOCKS 3
 #endif
 
-__global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon(const __grid_constant__ DevCtx C)
+// Transport consumer for photons (ELEC false) or electrons of one geometry
+// class G. The phantom-class kernel also takes the stage queue's new particles
+// (and hands those that start in the linac head to the head-class kernel);
+// the head-class kernel takes only its continuations. A particle outside the
+// class, or one whose step budget for this launch is spent, is re-queued for the
+// next wave with its state; the tally does not depend on where a track is split.
+template <bool ELEC, int G>
+__device__ __forceinline__ void transport_consumer(const DevCtx &C)
 {
+    constexpr int Q = ELEC ? ST_ELECTRON : ST_PHOTON;
+    constexpr bool HEAD = (G == GX_GEOM_HEAD);
+    constexpr int own = ELEC ? (HEAD ? GX_Q_EHCONT : GX_Q_ECONT) : (HEAD ? GX_Q_PHCONT : GX_Q_PCONT);
+    constexpr int other = ELEC ? (HEAD ? GX_Q_ECONT : GX_Q_EHCONT) : (HEAD ? GX_Q_PCONT : GX_Q_PHCONT);
     const uint32_t par = *C.wave & 1u;
-    const int qc_in = GX_Q_PCONT + (int)par, qc_out = GX_Q_PCONT + (int)(par ^ 1u);
+    // The head-class kernel runs first in a wave and hands particles to the
+    // phantom kernel of the same wave; the phantom kernel hands to the next wave.
+    const int qc_in = own + (int)par, qc_out = own + (int)(par ^ 1u);
+    const int qo_out = other + (int)(HEAD ? par : (par ^ 1u));
+    const int hq = HEAD ? qc_in : Q;
     const uint32_t n_cont = queue_len(C, qc_in);
-    const uint32_t n = n_cont + queue_len(C, ST_PHOTON);
-    Part p;
-    Rng r;
-    bool active = false, exhausted = false;
-    unsigned long long taken = 0, steps = 0;
-    uint32_t nst = 0;
-    for (;;) {
-        bool was = active;
-        active = refill<ST_PHOTON, false>(C, n_cont, n, qc_in, exhausted, active, p, r, nullptr, taken);
-        if (active && !was) nst = 0;
-        if (!__any_sync(0xffffffffu, active)) break;
-        if (active) {
-            steps++;
-            if (photon_step(C, p, r)) active = false;
-            else if (++nst >= C.photon_budget) { push_cont(C, qc_out, p, r, nullptr); active = false; }
-        }
-    }
-    block_stat_add(C, ST_PHOTON, taken);
-    block_stat_add(C, GX_NSTAGE, steps);
-    consumer_done(C, ST_PHOTON, qc_in);
-}
-
-__global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron(const __grid_constant__ DevCtx C)
-{
-    const uint32_t par = *C.wave & 1u;
-    const int qc_in = GX_Q_ECONT + (int)par, qc_out = GX_Q_ECONT + (int)(par ^ 1u);
-    const uint32_t n_cont = queue_len(C, qc_in);
-    const uint32_t n = n_cont + queue_len(C, ST_ELECTRON);
+    const uint32_t n = n_cont + (HEAD ? 0u : queue_len(C, Q));
+    const uint32_t budget = ELEC ? C.electron_budget : C.photon_budget;
     Part p;
     Rng r;
     EState s;
@@ -227,22 +216,50 @@ __global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron(const 
     uint32_t nst = 0;
     for (;;) {
         bool was = active;
-        active = refill<ST_ELECTRON, true>(C, n_cont, n, qc_in, exhausted, active, p, r, &s, taken);
+        active = refill<Q, ELEC>(C, hq, n_cont, n, qc_in, exhausted, active, p, r, &s, taken);
         if (active && !was) nst = 0;
         if (!__any_sync(0xffffffffu, active)) break;
         if (active) {
-            steps++;
-            if (electron_step(C, p, r, s)) active = false;
-            else if (++nst >= C.electron_budget) {
-                EStatePk k = pack_estate(s);
-                push_cont(C, qc_out, p, r, &k);
+            if (G != GX_GEOM_ALL && !in_geom_class<G>(p)) {
+                if (ELEC) { EStatePk k = pack_estate(s); push_cont(C, qo_out, p, r, &k); }
+                else push_cont(C, qo_out, p, r, nullptr);
                 active = false;
+            } else {
+                steps++;
+                bool done = ELEC ? electron_step<G>(C, p, r, s) : photon_step<G>(C, p, r);
+                if (done) active = false;
+                else if (++nst >= budget) {
+                    if (ELEC) { EStatePk k = pack_estate(s); push_cont(C, qc_out, p, r, &k); }
+                    else push_cont(C, qc_out, p, r, nullptr);
+                    active = false;
+                }
             }
         }
     }
-    block_stat_add(C, ST_ELECTRON, taken);
-    block_stat_add(C, GX_NSTAGE + 1, steps);
-    consumer_done(C, ST_ELECTRON, qc_in);
+    if (!HEAD) block_stat_add(C, Q, taken);
+    block_stat_add(C, GX_NSTAGE + (ELEC ? 1 : 0), steps);
+    if (HEAD) consumer_done(C, qc_in);
+    else consumer_done(C, Q, qc_in);
+}
+
+__global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon(const __grid_constant__ DevCtx C)
+{
+    transport_consumer<false, GX_GEOM_PHANTOM>(C);
+}
+
+__global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_head(const __grid_constant__ DevCtx C)
+{
+    transport_consumer<false, GX_GEOM_HEAD>(C);
+}
+
+__global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron(const __grid_constant__ DevCtx C)
+{
+    transport_consumer<true, GX_GEOM_PHANTOM>(C);
+}
+
+__global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_head(const __grid_constant__ DevCtx C)
+{
+    transport_consumer<true, GX_GEOM_HEAD>(C);
 }
 
 template <int Q>

@@ -54,7 +54,7 @@ typedef enum gegs_mode {
 
 typedef struct gegs_run_opts {
     int32_t mode;              /* gegs_mode */
-    uint32_t batch;            /* particles kept in flight (0 = default 4M; queue memory ~3.8 KB each) */
+    uint32_t batch;            /* particles kept in flight (0 = default 4M; queue memory ~5.2 KB each) */
     int32_t blocks_per_sm;     /* 0 = default */
     int32_t threads_per_block; /* 0 = default */
     uint32_t max_waves;        /* safety budget (0 = default) */
@@ -100,7 +100,7 @@ gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, con
  * gegs_run_noalloc transports histories [hist_begin, hist_end) like gegs_run
  * and adds to the same tally, but it allocates no device memory. Its event
  * queues, scheduler state and counters live in one fixed array compiled into
- * the library (about 21 MB, held on every GPU that loads the library until the
+ * the library (about 27 MB, held on every GPU that loads the library until the
  * process exits). Use it when the caller cannot allocate at run time:
  *   - a planning system or dose server that reserved the GPU's memory when it
  *     started, where a later cudaMalloc of gegs_run's queues (several GB at
