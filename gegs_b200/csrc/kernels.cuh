@@ -226,6 +226,7 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
                 active = false;
             } else {
                 steps++;
+                rng_window(C, r);
                 bool done = ELEC ? electron_step<G>(C, p, r, s) : photon_step<G>(C, p, r);
                 if (done) active = false;
                 else if (++nst >= budget) {
@@ -284,6 +285,7 @@ __global__ void __launch_bounds__(256) k_interact(const __grid_constant__ DevCtx
         Part p = load_part(&C.q.buf[Q][i]);
         Rng r;
         rng_load(r, p);
+        rng_window(C, r);
         trace_event(C, 1u, Q, p);
         run_interaction<Q>(C, p, r);
         taken++;
