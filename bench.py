@@ -240,12 +240,8 @@ def main():
         if dist is not None:
             import torch
 
-            class _Dev:
-                def __init__(self, ptr, n):
-                    self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i8", "data": (ptr, False),
-                                                     "version": 3}
-            t_dev = torch.as_tensor(_Dev(eng.tally_device_ptr(), eng.nvox), device=f"cuda:{local}")
-            dist.all_reduce(t_dev)
+            from gegs_b200.sharding import allreduce_tally_, tally_tensor
+            allreduce_tally_(tally_tensor(eng, f"cuda:{local}"))
             torch.cuda.synchronize()
         wall = time.perf_counter() - t0
     elapsed_s = sum(dev_ms) / 1e3
