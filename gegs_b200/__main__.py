@@ -1,0 +1,69 @@
+"""Command line: run a plan given in the reference's INI format.
+
+    python -m gegs_b200 -i plan.ini [--device N] [--max-histories N]
+
+Writes ``<output directory>/<output prefix>_DoseResults_NNNxNNNxNNN.bin``
+(raw float32 dose, x fastest, cGy when the plan is calibrated; the layout of
+the reference's write_dose, output.c:873-918) and ``<prefix>_log.txt``.
+All fields run in one transport call on the GPU; with output factors the
+fields run one by one and their energies are weighted before the dose
+conversion (CUDA_EGS.cu:1715-1735).
+"""
+from __future__ import annotations
+
+import argparse
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+
+def run_plan(ini, device=0, max_histories=None, out=sys.stdout):
+    from . import build as B
+    from . import io_formats as F
+    from .plan import load_plan
+    plan = load_plan(ini, max_histories=max_histories)
+    job = plan.job
+    B.build()
+    from .engine import Engine
+    eng = Engine(device)
+    eng.set_physics(job.physics)
+    eng.set_scene(job.scene())
+    t0 = time.perf_counter()
+    if all(abs(f - 1.0) < 1e-12 for f in plan.field_output_factors):
+        eng.run(0, job.histories)
+        energy = eng.tally().astype(np.float64)
+    else:
+        energy = np.zeros(eng.nvox, np.float64)
+        for f, of in zip(job.fields, plan.field_output_factors):
+            eng.reset_tally()
+            eng.run(int(f["hist_begin"]), int(f["hist_end"]))
+            energy += eng.tally().astype(np.float64) * of
+    wall = time.perf_counter() - t0
+    dose = energy * (2.0 ** -30) / job.voxel_mass() * plan.dose_unit
+    Path(plan.output_dir).mkdir(parents=True, exist_ok=True)
+    name = F.write_dose(plan.output_base, dose.astype(np.float32), plan.nx, plan.ny, plan.nz)
+    st = eng.stats()
+    lines = [f"plan {ini}", f"fields {len(job.fields)}, histories {job.histories}, phase-space particles {len(job.phsp)}",
+             f"media {job.media}", f"dose unit {plan.dose_unit:.4e}",
+             f"transport {wall:.3f} s ({job.histories / max(wall, 1e-9):.4g} histories/s), waves {st['waves']}",
+             f"dose file {name}"] + plan.log
+    Path(plan.output_base + "_log.txt").write_text("\n".join(lines) + "\n")
+    for l in lines:
+        print(l, file=out)
+    eng.close()
+    return name
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(prog="python -m gegs_b200")
+    ap.add_argument("-i", "--input", required=True, help="plan in the reference's INI format")
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--max-histories", type=int, default=None, help="cap the histories of each field")
+    a = ap.parse_args(argv)
+    run_plan(a.input, a.device, a.max_histories)
+
+
+if __name__ == "__main__":
+    main()

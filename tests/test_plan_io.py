@@ -1,0 +1,191 @@
+"""The drop-in boundary: the reference's input files and INI schema in, the
+``_DoseResults_NNNxNNNxNNN.bin`` dose grid out.
+
+A synthetic CT plan (the C3 workload on a small grid) is written to disk in
+the reference's formats (egsphant, egsphsp1, egsinp with CM DYNVMLC and CM
+JAWS SECJAWS, mlcinfo + mlcinp, INI); reading it back with ``load_plan`` must
+give the same transport job, so the oracle's tally for both is the same bit
+for bit. The GPU test runs the command line on that plan and checks the dose
+file against the oracle's tally converted the same way."""
+import numpy as np
+import pytest
+
+from gegs_b200 import geometry as G
+from gegs_b200 import io_formats as F
+from gegs_b200 import workloads as W
+from gegs_b200.plan import PlanError, load_plan, read_ini
+from gegs_b200.scene import PHSP_DTYPE
+
+DIMS = (24, 24, 12)
+PER_FIELD = 400
+
+
+def _job():
+    return W.config3(histories=5 * PER_FIELD, nphsp=3000, dims=DIMS)
+
+
+def _write_plan(tmp_path, job, extra=""):
+    d = tmp_path / "data"
+    d.mkdir()
+    p = job.phantom
+    F.write_egsphant(d / "head.egsphant", job.media, p["x_bounds"], p["y_bounds"], p["z_bounds"], p["voxel_med"],
+                     p["density"])
+    F.write_egsphsp1(d / "beam.egsphsp1", job.phsp, "MODE0")
+    (d / "VarianMLC.egsinp").write_text("TITLE\n" + F.dynvmlc_egsinp_text(job.meta["mlc"]) +
+                                        F.secjaws_egsinp_text(job.meta["jaws"]))
+    fields = []
+    for i, f in enumerate(job.fields):
+        name = f"field{i + 1}.mlcinp"
+        F.write_mlcinp(d / name, f["leaf_pos"])
+        x1, x2, y1, y2 = f["jaws"]
+        fields.append(dict(angle=f["angle"], x1=x1, x2=x2, y1=y1, y2=y2, mu=1, mlcinp=name))
+    F.write_mlcinfo(d / "plan.mlcinfo", fields)
+    ini = tmp_path / "plan.ini"
+    ini.write_text(f"""[General]
+output prefix = "T1"
+output directory = "out"
+histories = {PER_FIELD}
+
+[Data]
+data directory = "data"
+egsinp file = "VarianMLC.egsinp"
+pegs file = "700icru.pegs4dat"
+default medium = AIR700ICRU
+
+[Phase space]
+phsp file number = 1
+phase space file = "beam"
+z position = {job.beam['z_phsp']}
+
+[SecJaws]
+module SecJaws = On
+secjaws file = "VarianMLC.egsinp"
+
+[MLC]
+module MLC = On
+mlcinfo file = "plan.mlcinfo"
+
+[Block]
+module Block = Off
+
+[Wedge]
+module Wedge = Off
+
+[CTcreate]
+use ctcreate = No
+
+[Phantom]
+change coordinate = Yes
+egsphant file = "head.egsphant"
+isocenter location = 0 0 0
+source to isocenter = 100
+
+[Calibration]
+dose calibration = No
+{extra}""")
+    return ini
+
+
+def test_egsphant_round_trip(tmp_path):
+    job = _job()
+    p = job.phantom
+    F.write_egsphant(tmp_path / "a.egsphant", job.media, p["x_bounds"], p["y_bounds"], p["z_bounds"],
+                     p["voxel_med"], p["density"])
+    r = F.read_egsphant(tmp_path / "a.egsphant")
+    assert r["media"] == job.media and (r["nx"], r["ny"], r["nz"]) == DIMS
+    for k in ("x_bounds", "y_bounds", "z_bounds", "density"):
+        np.testing.assert_array_equal(r[k], np.asarray(p[k], np.float32))
+    np.testing.assert_array_equal(r["voxel_med"], p["voxel_med"])
+
+
+@pytest.mark.parametrize("mode", ["MODE0", "MODE2"])
+def test_egsphsp1_round_trip_and_parts(tmp_path, mode):
+    recs = _job().phsp[:1000]
+    F.write_egsphsp1(tmp_path / "b_p0.egsphsp1", recs[:600], mode)
+    F.write_egsphsp1(tmp_path / "b_p1.egsphsp1", recs[600:], mode)
+    h = F.read_egsphsp1_header(tmp_path / "b_p0.egsphsp1")
+    assert h["mode"] == mode and h["n"] == 600 and h["reclen"] == (28 if mode == "MODE0" else 32)
+    got = F.read_phase_space(str(tmp_path / "b"), 2)
+    assert got.dtype == PHSP_DTYPE
+    np.testing.assert_array_equal(got, recs)
+    np.testing.assert_array_equal(F.read_egsphsp1(tmp_path / "b_p1.egsphsp1", start=100, count=50), recs[700:750])
+
+
+def test_egsinp_modules_round_trip(tmp_path):
+    m, j = G.DynVMLC.synthetic(), G.SecJaws()
+    (tmp_path / "x.egsinp").write_text("a title\n:start geometry:\n" + F.secjaws_egsinp_text(j) +
+                                      F.dynvmlc_egsinp_text(m))
+    assert F.read_dynvmlc(tmp_path / "x.egsinp") == m
+    assert F.read_secjaws(tmp_path / "x.egsinp") == j
+    (tmp_path / "none.egsinp").write_text("no modules here\n")
+    with pytest.raises(ValueError):
+        F.read_dynvmlc(tmp_path / "none.egsinp")
+
+
+def test_mlcinfo_and_mlcinp_round_trip(tmp_path):
+    pos = np.random.default_rng(1).uniform(-3, 9, 120).astype(np.float32)
+    F.write_mlcinp(tmp_path / "f.mlcinp", pos)
+    np.testing.assert_array_equal(F.read_mlcinp(tmp_path / "f.mlcinp"), pos)
+    fl = [dict(angle=a, x1=-5, x2=5.5, y1=-4, y2=6, mu=mu, mlcinp=f"f{i}.mlcinp")
+          for i, (a, mu) in enumerate([(0, 100), (72.5, 50)])]
+    F.write_mlcinfo(tmp_path / "p.mlcinfo", fl)
+    got = F.read_mlcinfo(tmp_path / "p.mlcinfo")
+    assert [(g["angle"], g["x1"], g["x2"], g["y1"], g["y2"], g["mu"], g["mlcinp"]) for g in got] == \
+           [(f["angle"], f["x1"], f["x2"], f["y1"], f["y2"], f["mu"], f["mlcinp"]) for f in fl]
+
+
+def test_ini_reader_rules(tmp_path):
+    (tmp_path / "a.ini").write_text('[General]\nOutput Prefix = "V1"\n; comment\n[phantom]\nSource to isocenter = 100\n')
+    ini = read_ini(tmp_path / "a.ini")
+    assert ini["general"]["output prefix"] == "V1" and ini["phantom"]["source to isocenter"] == "100"
+
+
+def test_plan_from_files_is_the_same_job(tmp_path, oracle):
+    job = _job()
+    plan = load_plan(_write_plan(tmp_path, job), seed=job.meta["seed"])
+    pj = plan.job
+    assert (plan.nx, plan.ny, plan.nz) == DIMS and pj.media == job.media and pj.histories == job.histories
+    assert plan.output_base.endswith("out/T1") and plan.dose_unit == pytest.approx(1.6e-8)
+    np.testing.assert_array_equal(pj.physics, job.physics)
+    for k in ("voxel_med", "voxel_rhof", "density"):
+        np.testing.assert_array_equal(pj.phantom[k], job.phantom[k])
+    assert pj.phantom["other_med"] == job.phantom["other_med"]
+    np.testing.assert_array_equal(pj.phsp, job.phsp)
+    for a, b in zip(pj.fields, job.fields):
+        for k in ("hist_begin", "hist_end", "nrepeat", "cos_angle", "sin_angle"):
+            assert a[k] == b[k], k
+        for k in ("endnode", "jawsGeomY", "jawsGeomX", "boundMinY", "boundMinX"):
+            np.testing.assert_array_equal(a[k], b[k])
+    ref, _ = oracle.run(job.physics, job.scene(), 0, job.histories)
+    got, _ = oracle.run(pj.physics, pj.scene(), 0, pj.histories)
+    assert ref.sum() > 0
+    np.testing.assert_array_equal(got, ref)
+
+
+def test_plan_rejects_unsupported_modules(tmp_path):
+    job = _job()
+    ini = _write_plan(tmp_path, job)
+    txt = ini.read_text().replace("module Wedge = Off", "module Wedge = On")
+    ini.write_text(txt)
+    with pytest.raises(PlanError, match="Wedge"):
+        load_plan(ini)
+
+
+def test_dose_file_layout(tmp_path):
+    d = np.arange(24 * 24 * 12, dtype=np.float32)
+    name = F.write_dose(str(tmp_path / "P"), d, 24, 24, 12)
+    assert name.endswith("P_DoseResults_024x024x012.bin")
+    np.testing.assert_array_equal(F.read_dose(name).reshape(-1), d)
+
+
+@pytest.mark.gpu
+def test_command_line_writes_the_dose_grid(tmp_path, oracle):
+    from gegs_b200.__main__ import run_plan
+    job = _job()
+    ini = _write_plan(tmp_path, job, extra="")
+    name = run_plan(str(ini))
+    plan = load_plan(ini)
+    ref, _ = oracle.run(plan.job.physics, plan.job.scene(), 0, plan.job.histories)
+    want = (ref.astype(np.float64) * 2.0 ** -30 / plan.job.voxel_mass() * plan.dose_unit).astype(np.float32)
+    np.testing.assert_array_equal(F.read_dose(name).reshape(-1), want)
+    assert (tmp_path / "out" / "T1_log.txt").exists()
