@@ -78,9 +78,13 @@ struct __align__(16) Part {
     uint32_t sid_lo, sid_hi;
     int8_t charge, leafIndex, bank;
     uint8_t module;
-    uint8_t field, status, pad0, pad1;
+    uint8_t field, status;
+    uint16_t beamlet;       // beamlet of the history's primary (GX_NO_BEAMLET: none)
 };
 static_assert(sizeof(Part) == 64, "particle record must be 64 bytes");
+#define GX_NO_BEAMLET 0xFFFFu
+// copies of the beamlet gradient accumulator (lane-indexed, summed on the host)
+#define GX_GRAD_COPIES 32
 
 // 8-byte region record (medium, flags, density ratio); cuts come from the medium.
 struct __align__(8) Vox {
@@ -140,6 +144,13 @@ struct DevCtx {
     float2 boundaryXZ[4], boundaryYZ[4];
     int8_t module_order[8];
     uint32_t seed_lo, seed_hi;
+    // beamlets: tagging grid, fluence weights (null: 1) and, in a gradient
+    // replay, d(objective)/d(energy) per voxel and the per-beamlet accumulator
+    int bl_nx, bl_ny, nbeamlets;
+    float bl_x0, bl_y0, bl_dx, bl_dy;
+    const float *bl_weight;
+    const double *gvm;
+    double *grad;           // [GX_GRAD_COPIES][nbeamlets]; null: energy tally
 };
 
 // ---------------------------------------------------------------------------
@@ -326,9 +337,17 @@ __device__ __forceinline__ RegInfo region_info(const DevCtx &C, uint32_t region)
     return r;
 }
 
-__device__ __forceinline__ void escore(const DevCtx &C, uint32_t region, float energy)
+__device__ __forceinline__ void escore(const DevCtx &C, const Part &p, uint32_t region, float energy)
 {
     if (region < GX_VAC_AND_OTH) return;
+    if (C.grad) {
+        // gradient replay: d(objective)/d(beamlet weight) += energy * d(objective)/d(energy in voxel)
+        if (p.beamlet != GX_NO_BEAMLET) {
+            double g = (double)energy * __ldg(&C.gvm[region - GX_VAC_AND_OTH]);
+            if (g != 0.0) atomicAdd(&C.grad[(size_t)(threadIdx.x & (GX_GRAD_COPIES - 1)) * C.nbeamlets + p.beamlet], g);
+        }
+        return;
+    }
     long long q = __float2ll_rn(energy * 1073741824.0f);
     if (q != 0) atomicAdd(&C.tally[region - GX_VAC_AND_OTH], (unsigned long long)q);
 }

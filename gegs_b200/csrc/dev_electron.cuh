@@ -238,7 +238,7 @@ __device__ __forceinline__ void estate_init(EState &s)
 
 __device__ __forceinline__ void e_discard_below_cut(const DevCtx &C, Part &p, const RegInfo &rd, Rng &r)
 {
-    escore(C, p.region, (p.e - C.P->prm) * p.wt);
+    escore(C, p, p.region, (p.e - C.P->prm) * p.wt);
     if (p.charge > 0) annih_at_rest(C, p, rd, r);
 }
 
@@ -390,7 +390,7 @@ __device__ bool electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
     }
     if (idisc > 0) {
         p.region = 0;
-        escore(C, 0, (p.e + (float)p.charge * prm) * p.wt);
+        escore(C, p, 0, (p.e + (float)p.charge * prm) * p.wt);
         return true;
     }
     if (ustep <= 0.0f) ustep = 0.0f;
@@ -405,7 +405,7 @@ __device__ bool electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
         rd = region_info(C, irnew);
         if (eie <= rd.ecut) { e_discard_below_cut(C, p, rd, r); return true; }
         if (ustep != 0.0f && idisc < 0) {
-            escore(C, p.region, (p.e + (float)p.charge * prm) * p.wt);
+            escore(C, p, p.region, (p.e + (float)p.charge * prm) * p.wt);
             return true;
         }
         s.is_tstep = true;
@@ -462,7 +462,7 @@ __device__ bool electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
     irold = p.region;
     eie = eie - edep;
     p.e = eie;
-    escore(C, irold, edep * p.wt);
+    escore(C, p, irold, edep * p.wt);
     if (irnew == irl && eie <= rd.ecut) { e_discard_below_cut(C, p, rd, r); return true; }
     unsigned medold = medium;
     if (medium != GX_VACUUM) {
@@ -479,7 +479,7 @@ __device__ bool electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
     }
     if (eie <= rd.ecut) { e_discard_below_cut(C, p, rd, r); return true; }
     if (idisc < 0) {
-        escore(C, p.region, (p.e + (float)p.charge * prm) * p.wt);
+        escore(C, p, p.region, (p.e + (float)p.charge * prm) * p.wt);
         return true;
     }
     if (medium != medold) { s.is_tstep = true; return false; }
@@ -619,7 +619,7 @@ __device__ void moller(const DevCtx &C, Part p, Rng &r)
                             eii_sample(C, ish, iz, uj, p, rd, r, edep);
                             if (p.e < rd.ecut) edep += p.e - prm;
                             else push_spawn(C, ST_ELECTRON, p, r);
-                            escore(C, p.region, edep * p.wt);
+                            escore(C, p, p.region, edep * p.wt);
                             return;
                         }
                     }
@@ -628,7 +628,7 @@ __device__ void moller(const DevCtx &C, Part p, Rng &r)
         }
     }
     float te = P->te[medium];
-    if (ekin <= 2.0f * te) { escore(C, p.region, (p.e - prm) * p.wt); return; }
+    if (ekin <= 2.0f * te) { escore(C, p, p.region, (p.e - prm) * p.wt); return; }
     float t0 = ekin / rm;
     float e0 = t0 + 1.0f;
     float extrae = eie - P->thmoll[medium];
@@ -665,7 +665,7 @@ __device__ void moller(const DevCtx &C, Part p, Rng &r)
     uphi32(costhe, sinthe, cosphi, sinphi, p1);
     if (p1.e < rd.ecut) edep += p1.e - prm;
     else push_spawn(C, ST_ELECTRON, p1, r);
-    escore(C, p.region, edep * p.wt);
+    escore(C, p, p.region, edep * p.wt);
 }
 
 __device__ void brems(const DevCtx &C, Part p, Rng &r)
@@ -785,7 +785,7 @@ __device__ void brems(const DevCtx &C, Part p, Rng &r)
     p.e = ese;
     if (p.e < rd.ecut) edep += p.e - prm;
     else push_spawn(C, ST_ELECTRON, p, r);
-    escore(C, p.region, edep * p.wt);
+    escore(C, p, p.region, edep * p.wt);
 }
 
 __device__ void bhabha(const DevCtx &C, Part p, Rng &r)
@@ -846,7 +846,7 @@ __device__ void bhabha(const DevCtx &C, Part p, Rng &r)
         edep += p1.e - prm;
         if (p1.charge > 0) annih_at_rest(C, p1, rd, r);
     } else push_spawn(C, ST_ELECTRON, p1, r);
-    escore(C, p.region, edep * p.wt);
+    escore(C, p, p.region, edep * p.wt);
 }
 
 __device__ void annih(const DevCtx &C, Part p, Rng &r)
@@ -914,5 +914,5 @@ __device__ void annih(const DevCtx &C, Part p, Rng &r)
         if (p.e < rd.pcut) edep += p.e;
         else push_spawn(C, ST_PHOTON, p, r);
     }
-    escore(C, p.region, edep * p.wt);
+    escore(C, p, p.region, edep * p.wt);
 }

@@ -171,7 +171,7 @@ __device__ bool photon_step(const DevCtx &C, Part &p, Rng &r)
 {
     const gegs_physics *P = C.P;
     RegInfo rd = region_info(C, p.region);
-    if (p.e <= rd.pcut) { escore(C, p.region, p.e * p.wt); return true; }
+    if (p.e <= rd.pcut) { escore(C, p, p.region, p.e * p.wt); return true; }
     if (p.wt <= 0.0f) return true;
     float r1 = U(C, r);
     float dpmfp = -gx_log(r1);
@@ -200,14 +200,14 @@ __device__ bool photon_step(const DevCtx &C, Part &p, Rng &r)
     if (new_region == 0) {
         if (med == GX_VACUUM || p.leafIndex == GX_PASSMLC) idisc = 1; else idisc = -1;
     }
-    if (idisc > 0) { p.region = 0; escore(C, 0, p.e * p.wt); return true; }
+    if (idisc > 0) { p.region = 0; escore(C, p, 0, p.e * p.wt); return true; }
     p.x = p.x + p.u * tstep;
     p.y = p.y + p.v * tstep;
     p.z = p.z + p.w * tstep;
     if (med != GX_VACUUM) dpmfp = fmaxf_(0.0f, dpmfp - tstep / gmfp_val);
     unsigned old_medium = med;
     if (new_region != p.region) { p.region = new_region; rd = region_info(C, new_region); }
-    if (p.e <= rd.pcut || idisc < 0) { escore(C, p.region, p.e * p.wt); return true; }
+    if (p.e <= rd.pcut || idisc < 0) { escore(C, p, p.region, p.e * p.wt); return true; }
     if ((rd.med != old_medium) || (rd.med == GX_VACUUM) || (dpmfp >= GX_EPSGMFP)) return false;
     if (rd.flags & GEGS_F_RAYLEIGH) {
         r1 = U(C, r);
@@ -403,7 +403,7 @@ __device__ void compton(const DevCtx &C, Part p, Rng &r)
         }
         break;
     }
-    escore(C, p.region, edep * p.wt);
+    escore(C, p, p.region, edep * p.wt);
 }
 
 __device__ void photo(const DevCtx &C, Part p, Rng &r)
@@ -421,7 +421,7 @@ __device__ void photo(const DevCtx &C, Part p, Rng &r)
     if (peig < __ldg(&P->edge_energies[1])) {
         p.charge = -1;
         p.e = peig + prm;
-        if (p.e < rd.ecut) escore(C, p.region, (p.e - prm) * p.wt);
+        if (p.e < rd.ecut) escore(C, p, p.region, (p.e - prm) * p.wt);
         else push_spawn(C, ST_ELECTRON, p, r);
         return;
     }
@@ -527,7 +527,7 @@ __device__ void photo(const DevCtx &C, Part p, Rng &r)
         }
     }
     if (do_relax) relax(C, e_vac, k, iz, edep, p, rd, r);
-    escore(C, p.region, edep * p.wt);
+    escore(C, p, p.region, edep * p.wt);
 }
 
 __device__ void rayleigh(const DevCtx &C, Part p, Rng &r)
@@ -575,7 +575,7 @@ __device__ void rayleigh(const DevCtx &C, Part p, Rng &r)
     float sinthe = sqrtf(1.0f - costhe2);
     float cosphi, sinphi;
     uphi21(C, costhe, sinthe, cosphi, sinphi, p, r);
-    if (p.e < rd.pcut) escore(C, p.region, p.e * p.wt);
+    if (p.e < rd.pcut) escore(C, p, p.region, p.e * p.wt);
     else push_spawn(C, ST_PHOTON, p, r);
 }
 
@@ -602,7 +602,7 @@ __device__ void annih_at_rest(const DevCtx &C, Part &p, const RegInfo &rd, Rng &
         if (p.e < rd.pcut) edep += p.e;
         else push_spawn(C, ST_PHOTON, p, r);
     }
-    escore(C, p.region, edep * p.wt);
+    escore(C, p, p.region, edep * p.wt);
 }
 
 __device__ void pair_angle(const DevCtx &C, Rng &r, int use, float ese, float eig, unsigned medium, float &costhe, float &sinthe)
@@ -776,7 +776,7 @@ __device__ void pair(const DevCtx &C, Part p, Rng &r)
                 } else push_spawn(C, ST_ELECTRON, p1, r);
             }
         }
-        escore(C, p.region, edep * p.wt);
+        escore(C, p, p.region, edep * p.wt);
         return;
     }
     {
@@ -795,5 +795,5 @@ __device__ void pair(const DevCtx &C, Part p, Rng &r)
         edep += p1.e - prm;
         if (p1.charge > 0) annih_at_rest(C, p1, rd, r);
     } else push_spawn(C, ST_ELECTRON, p1, r);
-    escore(C, p.region, edep * p.wt);
+    escore(C, p, p.region, edep * p.wt);
 }

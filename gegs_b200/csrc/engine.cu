@@ -64,9 +64,17 @@ struct gegs_engine {
     unsigned long long ctx_gen = 1;
 
     // cached persistent graph
-    cudaGraphExec_t gexec = nullptr;
-    unsigned long long graph_gen = 0;
-    int graph_grid = 0, graph_threads = 0;
+    // cached persistent graphs: slot 0 forward transport, slot 1 gradient replay
+    int slot = 0;
+    cudaGraphExec_t gexec[2] = {};
+    unsigned long long graph_gen[2] = {};
+    int graph_grid[2] = {}, graph_threads[2] = {};
+
+    // beamlets
+    float *d_blw = nullptr;            // fluence weights
+    uint32_t nbeamlets = 0;
+    double *d_gvm = nullptr;           // d(objective)/d(energy) per voxel, for the replay
+    double *d_grad = nullptr;          // [GX_GRAD_COPIES][nbeamlets]
 
     gegs_run_stats last{};
 };
@@ -129,7 +137,8 @@ void gegs_destroy(gegs_engine *e)
     if (!e) return;
     cudaSetDevice(e->device);
     if (e->stream) cudaStreamSynchronize(e->stream);
-    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    for (int k = 0; k < 2; k++) if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
+    cudaFree(e->d_blw); cudaFree(e->d_gvm); cudaFree(e->d_grad);
     cudaFree(e->d_P); cudaFree(e->d_reg); cudaFree(e->d_xb); cudaFree(e->d_yb); cudaFree(e->d_zb);
     cudaFree(e->d_fields); cudaFree(e->d_cross); cudaFree(e->d_phsp); cudaFree(e->d_tally);
     cudaFree(e->d_err); cudaFree(e->d_stats); cudaFree(e->d_sched); cudaFree(e->d_qmeta);
@@ -247,6 +256,24 @@ gegs_status gegs_set_scene(gegs_engine *e, const gegs_scene *S)
     for (int i = 0; i < 8; i++) C.module_order[i] = S->module_order[i];
     C.seed_lo = (uint32_t)S->seed;
     C.seed_hi = (uint32_t)(S->seed >> 32);
+    // beamlet grid and fluence weights
+    uint64_t nbl = S->bl_nx > 0 && S->bl_ny > 0 ? (uint64_t)S->nfields * S->bl_nx * S->bl_ny : 0;
+    if (nbl >= GX_NO_BEAMLET) { e->err = "at most 65534 beamlets"; return GEGS_ERR_ARG; }
+    C.bl_nx = nbl ? S->bl_nx : 0; C.bl_ny = nbl ? S->bl_ny : 0; C.nbeamlets = (int)nbl;
+    C.bl_x0 = S->bl_x0; C.bl_y0 = S->bl_y0; C.bl_dx = S->bl_dx; C.bl_dy = S->bl_dy;
+    C.bl_weight = nullptr;
+    C.gvm = nullptr;
+    C.grad = nullptr;
+    if (nbl != e->nbeamlets) {
+        CK(realloc_dev(&e->d_blw, (size_t)nbl), "beamlet weights");
+        CK(realloc_dev(&e->d_grad, (size_t)nbl * GX_GRAD_COPIES), "beamlet gradient");
+        e->nbeamlets = (uint32_t)nbl;
+    }
+    if (nbl && S->bl_weight) {
+        CK(cudaMemcpy(e->d_blw, S->bl_weight, nbl * sizeof(float), cudaMemcpyHostToDevice), "beamlet weights H2D");
+        C.bl_weight = e->d_blw;
+    }
+    if (e->d_gvm) { cudaFree(e->d_gvm); e->d_gvm = nullptr; }
     e->have_scene = true;
     e->ctx_gen++;
     return GEGS_OK;
@@ -309,8 +336,10 @@ static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
 
 static gegs_status build_graph(gegs_engine *e, int grid, int threads)
 {
-    if (e->gexec && e->graph_gen == e->ctx_gen && e->graph_grid == grid && e->graph_threads == threads) return GEGS_OK;
-    if (e->gexec) { cudaGraphExecDestroy(e->gexec); e->gexec = nullptr; }
+    const int k = e->slot;
+    if (e->gexec[k] && e->graph_gen[k] == e->ctx_gen && e->graph_grid[k] == grid && e->graph_threads[k] == threads)
+        return GEGS_OK;
+    if (e->gexec[k]) { cudaGraphExecDestroy(e->gexec[k]); e->gexec[k] = nullptr; }
     cudaGraph_t g;
     CK(cudaGraphCreate(&g, 0), "graph create");
     cudaGraphConditionalHandle handle;
@@ -328,11 +357,11 @@ static gegs_status build_graph(gegs_engine *e, int grid, int threads)
     k_plan_cond<<<1, 1, 0, e->stream>>>(e->ctx, e->d_sched, handle);
     cudaGraph_t captured;
     CK(cudaStreamEndCapture(e->stream, &captured), "end capture");
-    CK(cudaGraphInstantiate(&e->gexec, g, 0), "graph instantiate");
+    CK(cudaGraphInstantiate(&e->gexec[k], g, 0), "graph instantiate");
     cudaGraphDestroy(g);
-    e->graph_gen = e->ctx_gen;
-    e->graph_grid = grid;
-    e->graph_threads = threads;
+    e->graph_gen[k] = e->ctx_gen;
+    e->graph_grid[k] = grid;
+    e->graph_threads[k] = threads;
     return GEGS_OK;
 }
 
@@ -375,7 +404,7 @@ extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hi
         if (st != GEGS_OK) return st;
         CK(cudaEventRecord(e->ev0, e->stream), "event");
         k_plan<<<1, 1, 0, e->stream>>>(e->ctx, e->d_sched);
-        CK(cudaGraphLaunch(e->gexec, e->stream), "graph launch");
+        CK(cudaGraphLaunch(e->gexec[e->slot], e->stream), "graph launch");
         CK(cudaEventRecord(e->ev1, e->stream), "event");
     } else if (o.mode == GEGS_MODE_TIMED) {
         // Same kernels as the persistent graph, launched wave by wave with an
@@ -705,5 +734,64 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
     if (errbits & GX_ERR_SOURCE) { e->err = "history outside every field range"; return GEGS_ERR_SOURCE; }
     if (errbits & GX_ERR_STEP_BUDGET) { e->err = "wave budget exhausted"; return GEGS_ERR_STEP_BUDGET; }
     if (hsr.pending) { e->err = "wave budget exhausted"; return GEGS_ERR_STEP_BUDGET; }
+    return GEGS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// beamlet weights and the gradient replay
+// ---------------------------------------------------------------------------
+extern "C" gegs_status gegs_set_beamlet_weights(gegs_engine *e, const float *w, uint32_t n)
+{
+    if (!e || !e->have_scene) return GEGS_ERR_ARG;
+    if (n != e->nbeamlets || (n && !w)) {
+        e->err = "gegs_set_beamlet_weights: the count must equal nfields * bl_nx * bl_ny of the scene";
+        return GEGS_ERR_ARG;
+    }
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    if (n) CK(cudaMemcpyAsync(e->d_blw, w, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, e->stream), "weights H2D");
+    CK(cudaStreamSynchronize(e->stream), "weights sync");
+    if (e->ctx.bl_weight != e->d_blw) { e->ctx.bl_weight = n ? e->d_blw : nullptr; e->ctx_gen++; }
+    return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_backward(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const double *voxel_grad,
+                                     double *beamlet_grad, uint32_t n, const gegs_run_opts *opts)
+{
+    if (!e || !e->have_scene || !voxel_grad || !beamlet_grad) return GEGS_ERR_ARG;
+    if (n != e->nbeamlets || n == 0) {
+        e->err = "gegs_backward: the scene has no beamlet grid, or n differs from its beamlet count";
+        return GEGS_ERR_ARG;
+    }
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    bool fresh = false;
+    if (!e->d_gvm) { CK(cudaMalloc(&e->d_gvm, e->nvox * sizeof(double)), "voxel gradient"); fresh = true; }
+    CK(cudaMemcpyAsync(e->d_gvm, voxel_grad, e->nvox * sizeof(double), cudaMemcpyHostToDevice, e->stream), "gvm H2D");
+    CK(cudaMemsetAsync(e->d_grad, 0, (size_t)n * GX_GRAD_COPIES * sizeof(double), e->stream), "grad reset");
+    // replay the histories with unit fluence weights, scoring into the gradient
+    DevCtx saved = e->ctx;
+    e->ctx.bl_weight = nullptr;
+    e->ctx.gvm = e->d_gvm;
+    e->ctx.grad = e->d_grad;
+    if (fresh) e->ctx_gen++;
+    gegs_run_opts o = {};
+    if (opts) o = *opts;
+    o.mode = GEGS_MODE_PERSISTENT;
+    e->slot = 1;
+    gegs_status st = gegs_run(e, hist_begin, hist_end, &o);
+    e->slot = 0;
+    DevCtx after = e->ctx;
+    e->ctx = saved;
+    e->ctx.q = after.q;                          // queue buffers may have been re-sized by the run
+    e->ctx.photon_budget = after.photon_budget;
+    e->ctx.electron_budget = after.electron_budget;
+    if (fresh) e->ctx_gen++;
+    if (st != GEGS_OK) return st;
+    std::vector<double> g((size_t)n * GX_GRAD_COPIES);
+    CK(cudaMemcpy(g.data(), e->d_grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost), "grad D2H");
+    for (uint32_t b = 0; b < n; b++) {
+        double acc = 0.0;
+        for (int k = 0; k < GX_GRAD_COPIES; k++) acc += g[(size_t)k * n + b];
+        beamlet_grad[b] = acc;
+    }
     return GEGS_OK;
 }

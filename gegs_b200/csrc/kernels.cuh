@@ -126,7 +126,19 @@ __device__ bool make_primary(const DevCtx &C, unsigned long long h, Part &p)
     p.hist_lo = (uint32_t)h;
     p.hist_hi = (uint32_t)(h >> 32);
     p.sid_lo = 0; p.sid_hi = 0; p.ctr = 0;
-    p.status = 0; p.pad0 = 0; p.pad1 = 0;
+    p.status = 0;
+    // beamlet: the bixel of the isocentre plane on the primary's straight line
+    p.beamlet = GX_NO_BEAMLET;
+    if (C.bl_nx > 0 && w > 0.0f) {
+        float t = (C.sid - C.z_phsp) / w;
+        float xi = rx + ru * t, yi = ry + rv * t;
+        float fx = (xi - C.bl_x0) / C.bl_dx, fy = (yi - C.bl_y0) / C.bl_dy;
+        if (fx >= 0.0f && fy >= 0.0f && fx < (float)C.bl_nx && fy < (float)C.bl_ny) {
+            int b = f * C.bl_nx * C.bl_ny + (int)fy * C.bl_nx + (int)fx;
+            p.beamlet = (uint16_t)b;
+            if (C.bl_weight) p.wt = wt * __ldg(&C.bl_weight[b]);
+        }
+    }
     return true;
 }
 

@@ -20,7 +20,7 @@ MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 
 EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
            "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_get_dose", "gegs_get_stats",
-           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version"]
+           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version"]
 
 
 TRACE_DTYPE = np.dtype([("kind_stage", "<u4"), ("hist_lo", "<u4"), ("sid_lo", "<u4"), ("sid_hi", "<u4"),
@@ -65,6 +65,8 @@ def load_library(path=None):
     L.gegs_set_phsp.argtypes = [vp, vp, C.c_uint64]
     L.gegs_run.argtypes = [vp, C.c_uint64, C.c_uint64, C.POINTER(RunOpts)]
     L.gegs_run_noalloc.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint32]
+    L.gegs_set_beamlet_weights.argtypes = [vp, vp, C.c_uint32]
+    L.gegs_backward.argtypes = [vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint32, C.POINTER(RunOpts)]
     L.gegs_reset_tally.argtypes = [vp]
     L.gegs_get_tally.argtypes = [vp, vp, C.c_uint64]
     L.gegs_get_dose.argtypes = [vp, vp, C.c_double, vp, C.c_uint64]
@@ -120,6 +122,21 @@ class Engine:
         self._keep = scene_holder
         self._check(self.L.gegs_set_scene(self.h, C.addressof(scene_holder.scene)))
         self.nvox = scene_holder.nvox
+        self.nbeamlets = getattr(scene_holder, "nbeamlets", 0)
+
+    def set_beamlet_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32).reshape(-1)
+        self._check(self.L.gegs_set_beamlet_weights(self.h, w.ctypes.data, w.size))
+
+    def backward(self, h0: int, h1: int, voxel_grad, batch: int = 0):
+        """d(objective)/d(beamlet weight) from d(objective)/d(energy per voxel, MeV)."""
+        g = np.ascontiguousarray(voxel_grad, np.float64).reshape(-1)
+        if g.size != self.nvox:
+            raise ValueError(f"voxel gradient has {g.size} entries for {self.nvox} voxels")
+        out = np.zeros(self.nbeamlets, np.float64)
+        o = RunOpts(MODE_PERSISTENT, batch, 0, 0, 0, 0, 0)
+        self._check(self.L.gegs_backward(self.h, h0, h1, g.ctypes.data, out.ctypes.data, out.size, C.byref(o)))
+        return out
 
     def set_phsp(self, recs: np.ndarray):
         r = np.ascontiguousarray(recs)

@@ -55,6 +55,8 @@ class Scene(C.Structure):
         ("nfields", C.c_int32), ("fields", C.POINTER(Field)),
         ("phsp", C.POINTER(PhspRecord)), ("nphsp", C.c_uint64),
         ("hownear_region_offset", C.c_int32), ("pad2_", C.c_int32), ("seed", C.c_uint64),
+        ("bl_nx", C.c_int32), ("bl_ny", C.c_int32), ("bl_x0", C.c_float), ("bl_y0", C.c_float),
+        ("bl_dx", C.c_float), ("bl_dy", C.c_float), ("bl_weight", C.POINTER(C.c_float)),
     ]
 
 
@@ -120,6 +122,19 @@ class SceneHolder:
         s.nphsp = len(ph)
         s.hownear_region_offset = hownear_region_offset
         s.seed = seed
+        bl = beam.get("beamlets")
+        if bl is not None:
+            s.bl_nx, s.bl_ny = int(bl["nx"]), int(bl["ny"])
+            s.bl_x0, s.bl_y0, s.bl_dx, s.bl_dy = bl["x0"], bl["y0"], bl["dx"], bl["dy"]
+            if nf * s.bl_nx * s.bl_ny >= 0xFFFF:
+                raise ValueError("at most 65534 beamlets")
+            if bl.get("weights") is not None:
+                w = np.ascontiguousarray(bl["weights"], np.float32).reshape(-1)
+                if w.size != nf * s.bl_nx * s.bl_ny:
+                    raise ValueError(f"{w.size} beamlet weights for {nf * s.bl_nx * s.bl_ny} beamlets")
+                self.keep.append(w)
+                s.bl_weight = _ptr(w, C.c_float)
+        self.nbeamlets = nf * s.bl_nx * s.bl_ny
         self.scene = s
         self.nvox = s.nx * s.ny * s.nz
         self.total_histories = max(int(f["hist_end"]) for f in fields)

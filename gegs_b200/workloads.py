@@ -270,4 +270,31 @@ def config3(histories=200_000_000, seed=SEED_BASE + 3, nphsp=10_000_000, dims=(2
                meta=dict(seed=seed, mlc=mlc, jaws=jaws))
 
 
-CONFIGS = {1: config1, 2: config2, 3: config3}
+def ellipsoid_mask(job, center, axes):
+    """Voxels of the phantom whose centres lie in the ellipsoid (cm, phantom frame)."""
+    p = job.phantom
+    cx = [(np.asarray(p[k][:-1], np.float64) + np.asarray(p[k][1:], np.float64)) / 2
+          for k in ("x_bounds", "y_bounds", "z_bounds")]
+    Z, Y, X = np.meshgrid(cx[2], cx[1], cx[0], indexing="ij")
+    r = ((X - center[0]) / axes[0]) ** 2 + ((Y - center[1]) / axes[1]) ** 2 + ((Z - center[2]) / axes[2]) ** 2
+    return (r <= 1.0).reshape(-1)
+
+
+def config4(histories=50_000_000, seed=SEED_BASE + 4, nphsp=10_000_000, dims=(256, 256, 120), nb=20, bixel=0.5):
+    """C4: the C3 plan with every field split into nb x nb beamlets of `bixel` cm at
+    the isocentre (fluence weights 1 + U(0, 0.2)), a seeded ellipsoidal target
+    (prescription 60 units) and organ (one-sided limit 20 units)."""
+    job = config3(histories=histories, nphsp=nphsp, dims=dims, seed=seed)
+    rng = np.random.default_rng(seed + 1000)
+    nf = len(job.fields)
+    weights = (1.0 + rng.uniform(0.0, 0.2, nf * nb * nb)).astype(np.float32)
+    half = nb * bixel / 2
+    job.beam["beamlets"] = dict(nx=nb, ny=nb, x0=-half, y0=-half, dx=bixel, dy=bixel, weights=weights)
+    j = lambda s: rng.normal(0.0, s)
+    job.meta["target"] = ellipsoid_mask(job, (j(0.3), j(0.3), j(0.5)), (2.5, 2.0, 3.0))
+    job.meta["organ"] = ellipsoid_mask(job, (3.5 + j(0.3), 0.5 + j(0.3), j(0.5)), (1.0, 1.5, 2.0))
+    job.name = "C4 CT head 5 fields, beamlet weights"
+    return job
+
+
+CONFIGS = {1: config1, 2: config2, 3: config3, 4: config4}

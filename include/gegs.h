@@ -122,6 +122,21 @@ gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, con
 #define GEGS_NOALLOC_MAX_BATCH 4096u
 gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, uint32_t batch);
 
+/* Beamlets (no counterpart in the reference; the scene's bl_* fields define
+ * the grid). gegs_set_beamlet_weights replaces the n = nfields*bl_nx*bl_ny
+ * fluence weights that multiply the weight of each tagged primary.
+ *
+ * gegs_backward returns d(objective)/d(weight) for every beamlet, given
+ * voxel_grad[v] = d(objective)/d(energy deposited in voxel v, MeV) on the
+ * host (nvox doubles; for a dose objective: dL/dD_v * dose_unit / mass_v).
+ * It replays histories [hist_begin, hist_end) from their RNG counters with
+ * unit fluence weights, adding energy * voxel_grad[v] of every deposit to the
+ * gradient of the deposit's beamlet, so no per-history deposit is stored. The
+ * tally is not touched. opts as for gegs_run (the persistent form is used). */
+gegs_status gegs_set_beamlet_weights(gegs_engine *e, const float *w, uint32_t n);
+gegs_status gegs_backward(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const double *voxel_grad,
+                          double *beamlet_grad, uint32_t n, const gegs_run_opts *opts);
+
 gegs_status gegs_reset_tally(gegs_engine *e);
 
 /* Copy the int64 tally (nvox entries) to host memory. */

@@ -84,6 +84,16 @@ typedef struct gegs_scene {
     int32_t hownear_region_offset;   /* 5: reference voxel decode in hownear_phantom; 6: corrected */
     int32_t pad2_;
     uint64_t seed;                   /* Philox key */
+
+    /* Beamlets (no counterpart in the reference): a grid of bl_nx x bl_ny
+     * bixels of bl_dx x bl_dy cm starting at (bl_x0, bl_y0) in the isocentre
+     * plane of the beam frame, the same for every field. A primary is tagged
+     * with the bixel its straight line from the phase-space plane crosses;
+     * beamlet index = field * bl_nx * bl_ny + iy * bl_nx + ix. Its weight is
+     * multiplied by bl_weight[index] (NULL: weights 1). bl_nx = 0: no beamlets. */
+    int32_t bl_nx, bl_ny;
+    float bl_x0, bl_y0, bl_dx, bl_dy;
+    const float *bl_weight;
 } gegs_scene;
 
 #endif /* GEGS_SCENE_H */

@@ -82,6 +82,17 @@ static int make_primary(const gegs_scene *S, uint64_t h, ora_particle *p)
     p->v = rec->v;
     p->w = w;
     p->dnear = INFI_DIST;
+    /* beamlet fluence weight (no counterpart in the reference): the bixel of the
+     * isocentre plane on the primary's straight line; same arithmetic as the GPU */
+    if (S->bl_nx > 0 && w > 0.0f) {
+        float t = (S->source_to_isocenter - S->z_phsp) / w;
+        float xi = rec->x + rec->u * t, yi = rec->y + rec->v * t;
+        float fx = (xi - S->bl_x0) / S->bl_dx, fy = (yi - S->bl_y0) / S->bl_dy;
+        if (fx >= 0.0f && fy >= 0.0f && fx < (float)S->bl_nx && fy < (float)S->bl_ny) {
+            int b = f * S->bl_nx * S->bl_ny + (int)fy * S->bl_nx + (int)fx;
+            if (S->bl_weight) p->wt = wt * S->bl_weight[b];
+        }
+    }
     p->rng.hist_lo = (uint32_t)h;
     p->rng.hist_hi = (uint32_t)(h >> 32);
     p->status = q == 0 ? p_photon_step : e_electron_step;
