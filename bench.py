@@ -131,6 +131,47 @@ def cpu_histories_per_s(job, seconds=15.0, threads=None):
     return n2 / dt, n2, dt, threads
 
 
+def c4_gradient(args, eng):
+    """C4 (CT head, 5 fields x 20 x 20 beamlets of 5 mm): time of one forward and of
+    the replay backward, the cost of finite differences over every beamlet, and a
+    common-random-number finite-difference check on 4 beamlets."""
+    import torch
+
+    from gegs_b200 import workloads as W
+    from gegs_b200.differentiable import BeamletModel, beamlet_dose, fd_gradient, objective
+    job = W.config4(histories=args.c4_histories, nphsp=args.nphsp)
+    eng.set_physics(job.physics)
+    eng.set_scene(job.scene())
+    target, organ = job.meta["target"], job.meta["organ"]
+    loss = lambda d: objective(d, target, organ)
+    w0 = job.beam["beamlets"]["weights"].astype(np.float64)
+    model = BeamletModel(eng, job)
+    model.calibrate(w0, target, 50.0)
+    fwd, bwd = [], []
+    for _ in range(2):
+        w = torch.tensor(w0, requires_grad=True)
+        L = loss(beamlet_dose(w, model))
+        fwd.append(model.forward_ms)
+        L.backward()
+        bwd.append(model.backward_ms)
+    g_full = w.grad.numpy()
+    small = BeamletModel(eng, job, 0, args.c4_fd_histories, dose_unit=model.unit)
+    w = torch.tensor(w0, requires_grad=True)
+    loss(beamlet_dose(w, small)).backward()
+    g = w.grad.numpy()
+    pick = np.argsort(-np.abs(g))[[0, 10, 100, 400]]
+    fd = fd_gradient(small, w0, pick, loss, delta=0.05)
+    f_ms, b_ms = min(fwd), min(bwd)
+    return {"workload": f"C4 CT head 256x256x120, 5 fields x 20x20 beamlets of 5 mm, {job.histories} histories",
+            "beamlets": int(model.nb), "forward_ms": f_ms, "backward_ms": b_ms, "backward_over_forward": b_ms / f_ms,
+            "gradient_ms": f_ms + b_ms, "fd_all_beamlets_ms": 2 * model.nb * f_ms,
+            "fd_over_gradient": 2 * model.nb * f_ms / (f_ms + b_ms),
+            "fd_check": {"histories": args.c4_fd_histories, "beamlets": [int(b) for b in pick],
+                         "replay": [float(x) for x in g[pick]], "fd": [float(x) for x in fd],
+                         "max_rel_err": float(np.max(np.abs(g[pick] - fd) / np.abs(fd).max()))},
+            "grad_norm": float(np.linalg.norm(g_full))}
+
+
 def make_job(args, histories):
     from gegs_b200 import workloads as W
     return W.config3(histories=histories, nphsp=args.nphsp)
@@ -185,6 +226,11 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--plain-histories", type=int, default=2_000_000,
+                    help="histories of the plain-form comparison (0: skip)")
+    ap.add_argument("--c4-histories", type=int, default=50_000_000,
+                    help="forward/backward histories of the C4 gradient measurement (0: skip)")
+    ap.add_argument("--c4-fd-histories", type=int, default=5_000_000)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -303,8 +349,11 @@ def main():
     sig = None
     if args.steps >= 3:
         x = np.diff(np.concatenate([np.zeros((1, eng.nvox), np.int64), np.stack(snaps)]), axis=0).astype(np.float64)
+        x = x / job.voxel_mass()[None, :]          # dose per batch (energy / mass)
         mean = x.mean(axis=0)
-        sel = mean > 0.5 * mean.max()
+        # in the patient: voxels of density >= 0.1 g/cm^3 (air voxels' dose is noise-dominated)
+        body = job.phantom["density"].reshape(-1) >= 0.1
+        sel = body & (mean > 0.5 * mean[body].max())
         se = x[:, sel].std(axis=0, ddof=1) / np.sqrt(x.shape[0])
         rel = float(np.mean(se / mean[sel]))
         sig = rel
@@ -312,6 +361,22 @@ def main():
     if sig:
         n_done = H * args.steps * world
         t1pct = (n_done * (sig / 0.01) ** 2) / value
+
+    # ---- the plain form at the reference's launch shape, same histories ------
+    plain = None
+    if args.plain_histories > 0:
+        hp = args.plain_histories
+        pst = eng.run(0, hp, mode=MODE_PLAIN, batch=480_000, blocks_per_sm=5, threads=128)
+        qst = eng.run(0, hp, **dict(ropt, mode=MODE_PERSISTENT))
+        plain = {"histories": hp, "launch": "5 blocks/SM x 128 threads, 480000 histories per batch, host sync + "
+                                            "counter read-back after every kernel (CUDA_EGS.cu:226-365, 498-799)",
+                 "value": hp / pst["device_ms"] * 1e3, "persistent_value": hp / qst["device_ms"] * 1e3,
+                 "persistent_over_plain": pst["device_ms"] / qst["device_ms"],
+                 "note": "both forms give the same tally bit for bit, so equal histories give equal sigma "
+                         "and gamma; the ratio is the time-to-1% ratio"}
+
+    # ---- C4: beamlet gradient by replay vs forward and finite differences ---
+    grad = c4_gradient(args, eng) if args.c4_histories > 0 else None
 
     cpu = None
     if not args.no_cpu:
@@ -341,7 +406,10 @@ def main():
         "cpu_baseline": cpu,
         "gpu_launches": int(sum(launches_per_step)),
         "clocks": clk.summary(),
+        "plain_form": plain,
+        "gradient": grad,
         "stat_uncertainty": {"mean_rel_se_above_50pct_dmax": sig, "batches": args.steps,
+                             "voxels": "density >= 0.1 g/cm3 with batch-mean dose > 50 % of its maximum",
                              "time_to_1pct_s": t1pct},
         "device_stats": {"processed": stats[-1]["processed"], "photon_steps": stats[-1]["photon_steps"],
                          "electron_steps": stats[-1]["electron_steps"], "waves": stats[-1]["waves"]},

@@ -236,11 +236,14 @@ __device__ float ray_intersect_polygon(float2 p0, float2 v, const float2 *poly, 
         float2 b = LOCAL ? poly[j] : ld2(&poly[j]);
         float tmp1 = v.x * (b.y - a.y) - v.y * (b.x - a.x);
         if (tmp1 != 0) {
-            float dist = ((b.x - a.x) * (p0.y - a.y) - (b.y - a.y) * (p0.x - a.x)) / tmp1;
+            // the edge parameter first: most edges fail it, and then the distance is not needed
             float u = ((a.x - p0.x) * v.y - (a.y - p0.y) * v.x) / tmp1;
-            if (dist >= 0 && (u >= 0) && (u < 1)) {
-                count++;
-                if (dist < minDist) minDist = dist;
+            if ((u >= 0) && (u < 1)) {
+                float dist = ((b.x - a.x) * (p0.y - a.y) - (b.y - a.y) * (p0.x - a.x)) / tmp1;
+                if (dist >= 0) {
+                    count++;
+                    if (dist < minDist) minDist = dist;
+                }
             }
         }
     }
@@ -453,30 +456,36 @@ __device__ uint32_t howfar_secjaws_x(const DevCtx &C, Part &p, float &t)
 __device__ __forceinline__ float dist2p(float2 v, float2 w) { return (v.x - w.x) * (v.x - w.x) + (v.y - w.y) * (v.y - w.y); }
 __device__ __forceinline__ float distp(float2 v, float2 w) { return sqrtf((v.x - w.x) * (v.x - w.x) + (v.y - w.y) * (v.y - w.y)); }
 
-__device__ float point_dist_to_segment(float2 p, float2 v, float2 w)
+// Squared distance whose sqrtf is point_dist_to_segment(p, v, w), term for term.
+__device__ __forceinline__ float point_dist2_to_segment(float2 p, float2 v, float2 w)
 {
     float l2 = dist2p(v, w);
-    if (l2 == 0) return distp(p, v);
+    if (l2 == 0) return dist2p(p, v);
     float t = ((p.x - v.x) * (w.x - v.x) + (p.y - v.y) * (w.y - v.y)) / l2;
-    if (t < 0) return distp(p, v);
-    if (t > 1) return distp(p, w);
+    if (t < 0) return dist2p(p, v);
+    if (t > 1) return dist2p(p, w);
     float2 a = make_float2(v.x + t * (w.x - v.x), v.y + t * (w.y - v.y));
-    return distp(p, a);
+    return dist2p(p, a);
 }
 
+// Minimum edge distance of the polygon, capped at 1e9 (pointMinDistToPolygon,
+// geom.cu:1175-1191). sqrtf is correctly rounded and monotonic, so the
+// minimum of the edges' sqrtf equals sqrtf of the minimum squared distance:
+// one square root per polygon instead of one per edge, same result.
 template <bool LOCAL>
 __device__ float point_min_dist_to_polygon(float2 p0, const float2 *poly, int n)
 {
-    float minDist = 1e9f;
+    float min2 = __int_as_float(0x7f800000);
     for (int i = 0; i < n; i++) {
         int j = i + 1;
         if (j >= n) j = 0;
         float2 a = LOCAL ? poly[i] : ld2(&poly[i]);
         float2 b = LOCAL ? poly[j] : ld2(&poly[j]);
-        float d = point_dist_to_segment(p0, a, b);
-        if (d < minDist) minDist = d;
+        float d2 = point_dist2_to_segment(p0, a, b);
+        if (d2 < min2) min2 = d2;
     }
-    return minDist;
+    float d = sqrtf(min2);
+    return d < 1e9f ? d : 1e9f;
 }
 
 __device__ void hownear_mlc(const DevCtx &C, Part &p, float &tperp)
