@@ -337,15 +337,21 @@ __device__ __forceinline__ RegInfo region_info(const DevCtx &C, uint32_t region)
     return r;
 }
 
+// Gradient replay: d(objective)/d(beamlet weight) += energy * d(objective)/d(energy in the voxel).
+// Out of line: only the replay reaches it, and inlined at every scoring site it
+// would enlarge the forward kernels.
+__device__ __noinline__ void escore_grad(const DevCtx &C, uint32_t beamlet, uint32_t region, float energy)
+{
+    if (beamlet == GX_NO_BEAMLET) return;
+    double g = (double)energy * __ldg(&C.gvm[region - GX_VAC_AND_OTH]);
+    if (g != 0.0) atomicAdd(&C.grad[(size_t)(threadIdx.x & (GX_GRAD_COPIES - 1)) * C.nbeamlets + beamlet], g);
+}
+
 __device__ __forceinline__ void escore(const DevCtx &C, const Part &p, uint32_t region, float energy)
 {
     if (region < GX_VAC_AND_OTH) return;
     if (C.grad) {
-        // gradient replay: d(objective)/d(beamlet weight) += energy * d(objective)/d(energy in voxel)
-        if (p.beamlet != GX_NO_BEAMLET) {
-            double g = (double)energy * __ldg(&C.gvm[region - GX_VAC_AND_OTH]);
-            if (g != 0.0) atomicAdd(&C.grad[(size_t)(threadIdx.x & (GX_GRAD_COPIES - 1)) * C.nbeamlets + p.beamlet], g);
-        }
+        escore_grad(C, p.beamlet, region, energy);
         return;
     }
     long long q = __float2ll_rn(energy * 1073741824.0f);
