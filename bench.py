@@ -93,12 +93,13 @@ class ClockSampler:
 
 
 def traffic_from_profile(kind):
-    """DRAM bytes per launch of one kernel (scaled to the bench's launch size)
-    from the committed ncu summary ``profiles/<kind>_kernel_c3.md``."""
-    p = ROOT / "profiles" / f"{kind}_kernel_c3.md"
+    """DRAM bytes per transport step of the photon or electron kernels, from the
+    committed ncu summary ``profiles/transport_kernels_c3.md`` (all launches of
+    one run, DRAM read + write over the run's steps)."""
+    p = ROOT / "profiles" / "transport_kernels_c3.md"
     if not p.exists():
         return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+    m = re.search(rf"{kind}_dram_bytes_per_step:\s*([0-9.eE+-]+)", p.read_text())
     return float(m.group(1)) if m else None
 
 
@@ -334,16 +335,26 @@ def main():
     eng.set_phsp(job.phsp)
     tst = eng.run(0, H // 4, **dict(ropt, mode=MODE_TIMED))
     kinds = ["photon", "compton", "photo", "rayleigh", "pair", "electron", "moller", "brems", "bhabha", "annih",
-             "source", "planner"]
-    share = np.array(tst["stage_ms"][:12])
-    dom = int(np.argmax(share[:10]))
-    launches = max(1, tst["stage_launches"][dom])
+             "source", "planner", "photon_jaws", "electron_jaws", "photon_mlc", "electron_mlc"]
+    ms = np.array(tst["stage_ms"][:16])
+    # a transport stage runs as three launches per wave (jaws, MLC and phantom kernels)
+    groups = {k: [i] for i, k in enumerate(kinds[:10])}
+    groups["photon"] = [0, 12, 14]
+    groups["electron"] = [5, 13, 15]
+    stage_ms = {k: float(ms[idx].sum()) for k, idx in groups.items()}
+    dom_name = max(stage_ms, key=stage_ms.get)
+    dom = kinds.index(dom_name)
+    launches = max(1, tst["stage_launches"][dom])              # waves that ran this stage
     per_stage_bytes, ost = algorithmic_bytes(job, sample=20000)
     alg_bytes_per_launch = per_stage_bytes[dom] * (H // 4) / launches
-    avg_launch_s = tst["stage_ms"][dom] / 1e3 / launches
+    avg_launch_s = stage_ms[dom_name] / 1e3 / launches
     peak, peak_kind = hbm_peak()
     achieved = alg_bytes_per_launch / avg_launch_s / 1e9
-    tr = traffic_from_profile(kinds[dom])
+    steps_key = {"photon": "photon_steps", "electron": "electron_steps"}.get(dom_name)
+    per_step = traffic_from_profile(dom_name)
+    tr = per_step * tst[steps_key] / launches if (per_step is not None and steps_key) else None
+    total_ms = float(ms[[i for i in range(16) if i != 11]].sum())
+    share = {k: float(ms[i] / total_ms) for i, k in enumerate(kinds) if i != 11}
 
     # ---- batch-method statistical uncertainty -> time to 1 % ----------------
     sig = None
@@ -384,8 +395,8 @@ def main():
         cpu = {"value": crate, "unit": "histories/s", "cores": cores, "kind": "port",
                "sample": f"{cn} C3 histories in {cdt:.1f} s on {cores} host threads (CPU oracle, same inputs)"}
     # per step: the first planner launch, then per wave the source, the stage kernels (the
-    # persistent form runs photon and electron transport as phantom + linac-head kernels) and the planner
-    per_wave = 12 if args.mode == "plain" else 14
+    # persistent form runs photon and electron transport as jaws + MLC + phantom kernels) and the planner
+    per_wave = 12 if args.mode == "plain" else 16
     launches_per_step = [1 + per_wave * (st["waves"] - 1) for st in stats]
     line = {
         "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": world, "steps": args.steps,
@@ -398,11 +409,11 @@ def main():
                    "l2": "working set (63 MB region table + 63 MB int64 tally + event queues) exceeds the 126 MB L2; no flush"},
         "e2e": {"value": e2e, "unit": "histories/s", "h2d_bytes_per_step": rec_per_step * 28,
                 "d2h_bytes_per_step": eng.nvox * 8},
-        "roofline": {"bound": "hbm", "kernel": kinds[dom], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": tr,
+        "roofline": {"bound": "hbm", "kernel": f"{dom_name} transport (k_{dom_name}_jaws + k_{dom_name}_mlc + k_{dom_name}, one wave)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": tr,
                      "alg_bytes_per_launch": alg_bytes_per_launch, "avg_launch_ms": avg_launch_s * 1e3,
-                     "kernel_share": {k: float(v / share[:11].sum()) for k, v in zip(kinds[:11], share[:11])}},
+                     "kernel_share": share},
         "cpu_baseline": cpu,
         "gpu_launches": int(sum(launches_per_step)),
         "clocks": clk.summary(),

@@ -4,7 +4,9 @@
 
 Writes ``<output directory>/<output prefix>_DoseResults_NNNxNNNxNNN.bin``
 (raw float32 dose, x fastest, cGy when the plan is calibrated; the layout of
-the reference's write_dose, output.c:873-918) and ``<prefix>_log.txt``.
+the reference's write_dose, output.c:873-918), ``<prefix>_log.txt``, the
+interpolated grid ``<prefix>_Interpolate_NNNxNNNxNNN.bin`` when [Interpolation]
+asks for it, and the point dose of [Dose output] in the log.
 All fields run in one transport call on the GPU; with output factors the
 fields run one by one and their energies are weighted before the dose
 conversion (CUDA_EGS.cu:1715-1735).
@@ -45,10 +47,26 @@ def run_plan(ini, device=0, max_histories=None, out=sys.stdout):
     Path(plan.output_dir).mkdir(parents=True, exist_ok=True)
     name = F.write_dose(plan.output_base, dose.astype(np.float32), plan.nx, plan.ny, plan.nz)
     st = eng.stats()
+    extra = []
+    p = job.phantom
+    bounds = (p["x_bounds"], p["y_bounds"], p["z_bounds"])
+    if "interp" in plan.post:
+        from .postprocess import interp_dose, write_interp
+        ip = plan.post["interp"]
+        grid = interp_dose(dose.astype(np.float32), *bounds, ip["start"], ip["sizes"], ip["dims"], device=device)
+        extra.append(f"interpolated dose {write_interp(plan.output_base, grid)}")
+    if "point" in plan.post:
+        from .postprocess import point_dose
+        pt = plan.post["point"]
+        v = point_dose(dose.astype(np.float32), *bounds, pt["pos"])
+        msg = f"absolute dose at ({pt['pos'][0]:.2f}, {pt['pos'][1]:.2f}, {pt['pos'][2]:.2f}) = {v:.4g}"
+        if pt["measured"]:
+            msg += f" (measured {pt['measured']:.4g}, ratio {v / pt['measured']:.4f})"
+        extra.append(msg)
     lines = [f"plan {ini}", f"fields {len(job.fields)}, histories {job.histories}, phase-space particles {len(job.phsp)}",
              f"media {job.media}", f"dose unit {plan.dose_unit:.4e}",
              f"transport {wall:.3f} s ({job.histories / max(wall, 1e-9):.4g} histories/s), waves {st['waves']}",
-             f"dose file {name}"] + plan.log
+             f"dose file {name}"] + extra + plan.log
     Path(plan.output_base + "_log.txt").write_text("\n".join(lines) + "\n")
     for l in lines:
         print(l, file=out)

@@ -38,7 +38,7 @@ def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
     if not force and not needs_build():
         return LIB
     nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, "-o", str(LIB), str(SRC / "engine.cu")]
+    cmd = [nvcc, *NVCC_FLAGS, "-o", str(LIB), str(SRC / "engine.cu"), str(SRC / "postproc.cu")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     tmp = LIB.with_suffix(".so.tmp")

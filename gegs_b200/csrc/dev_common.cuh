@@ -40,15 +40,16 @@ static_assert(sizeof(gegs_field) % 16 == 0, "field record size");
 #define GX_MXGE GEGS_MXGE
 #define GX_MXEKE GEGS_MXEKE
 #define GX_NSTAGE 10
-// queues: 10 event stages, then ping-pong continuation queues that the
-// step-budgeted consumers re-queue into: photons in the phantom (10, 11) and in
-// the linac head (12, 13), electrons in the phantom (14, 15) and in the head
-// (16, 17). Electron continuations carry their step state (estate[qid - 14]).
+// queues: 10 event stages, then per particle type one ping-pong pair of
+// continuation queues for each geometry class in beam order (0 jaws, 1 MLC,
+// 2 phantom): photons 10..15, electrons 16..21 (pair = type base + 2 * class).
+// The step-budgeted consumers re-queue into them; electron continuations carry
+// their step state (estate[qid - GX_Q_ECONT]).
+#define GX_NCLASS 3
 #define GX_Q_PCONT 10
-#define GX_Q_PHCONT 12
-#define GX_Q_ECONT 14
-#define GX_Q_EHCONT 16
-#define GX_NQ 18
+#define GX_Q_ECONT 16
+#define GX_NQ 22
+#define GX_NESTATE 6
 #define GX_LOOP_CAP 1000
 #define GX_EPSGMFP 1.e-5f
 #define GX_EPSEMFP 1.e-5f
@@ -112,7 +113,7 @@ struct __align__(16) EStatePk {
 struct QueueSet {
     Part *buf[GX_NQ];
     uint32_t cap[GX_NQ];
-    EStatePk *estate[4];  // state of the four electron continuation queues
+    EStatePk *estate[GX_NESTATE];  // state of the electron continuation queues
     uint32_t *count;      // [GX_NQ] items queued
     uint32_t *head;       // [GX_NQ] items taken by the running consumer
     uint32_t *done;       // [GX_NQ] finished blocks of the running consumer

@@ -594,19 +594,28 @@ __device__ __forceinline__ void hownear(const DevCtx &C, Part &p, float &tperp, 
 }
 
 // Geometry classes: a consumer kernel compiled for one class contains only that
-// class's geometry code (phantom voxels, or jaws + MLC of the linac head), which
-// keeps the code a divergent warp runs small. A particle whose module is outside
-// the class is handed to the other class's kernel between steps.
+// class's geometry code -- the secondary jaws, the MLC, or the phantom voxels --
+// which keeps the code a divergent warp runs small. Classes are numbered in beam
+// order; a particle whose module is outside the class is handed to the other
+// class's kernel between steps. GX_GEOM_ALL compiles every module (plain form).
 #define GX_GEOM_ALL 0
-#define GX_GEOM_PHANTOM 1
-#define GX_GEOM_HEAD 2
+#define GX_GEOM_JAWS 1
+#define GX_GEOM_MLC 2
+#define GX_GEOM_PHANTOM 3
+
+// class of a module (unsupported modules fall in the jaws class, whose
+// geometry dispatch reports them)
+__device__ __forceinline__ int geom_class_of(uint8_t module)
+{
+    if (module == GEGS_M_PHANTOM) return GX_GEOM_PHANTOM;
+    if (module == GEGS_M_VARMLC) return GX_GEOM_MLC;
+    return GX_GEOM_JAWS;
+}
 
 template <int G>
 __device__ __forceinline__ bool in_geom_class(const Part &p)
 {
-    if (G == GX_GEOM_PHANTOM) return p.module == GEGS_M_PHANTOM;
-    if (G == GX_GEOM_HEAD) return p.module != GEGS_M_PHANTOM;
-    return true;
+    return G == GX_GEOM_ALL || geom_class_of(p.module) == G;
 }
 
 template <int G>
@@ -616,13 +625,11 @@ __device__ __forceinline__ uint32_t howfar_g(const DevCtx &C, Part &p, float &t,
     ok = true;
     if (G == GX_GEOM_PHANTOM) {
         if (p.module == GEGS_M_PHANTOM) return howfar_phantom(C, p, t);
+    } else if (G == GX_GEOM_MLC) {
+        if (p.module == GEGS_M_VARMLC) return howfar_mlc(C, p, t);
     } else {
-        switch (p.module) {
-        case GEGS_M_VARMLC: return howfar_mlc(C, p, t);
-        case GEGS_M_SECJAWY: return howfar_secjaws_y(C, p, t);
-        case GEGS_M_SECJAWX: return howfar_secjaws_x(C, p, t);
-        default: break;
-        }
+        if (p.module == GEGS_M_SECJAWY) return howfar_secjaws_y(C, p, t);
+        if (p.module == GEGS_M_SECJAWX) return howfar_secjaws_x(C, p, t);
     }
     ok = false;
     return 0;
@@ -635,13 +642,11 @@ __device__ __forceinline__ void hownear_g(const DevCtx &C, Part &p, float &tperp
     ok = true;
     if (G == GX_GEOM_PHANTOM) {
         if (p.module == GEGS_M_PHANTOM) { hownear_phantom(C, p, tperp); return; }
+    } else if (G == GX_GEOM_MLC) {
+        if (p.module == GEGS_M_VARMLC) { hownear_mlc(C, p, tperp); return; }
     } else {
-        switch (p.module) {
-        case GEGS_M_VARMLC: hownear_mlc(C, p, tperp); return;
-        case GEGS_M_SECJAWY: hownear_secjaws_y(C, p, tperp); return;
-        case GEGS_M_SECJAWX: hownear_secjaws_x(C, p, tperp); return;
-        default: break;
-        }
+        if (p.module == GEGS_M_SECJAWY) { hownear_secjaws_y(C, p, tperp); return; }
+        if (p.module == GEGS_M_SECJAWX) { hownear_secjaws_x(C, p, tperp); return; }
     }
     ok = false;
     tperp = 0;

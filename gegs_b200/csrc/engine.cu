@@ -12,8 +12,9 @@
 namespace {
 
 // queue capacity per history in flight, per stage
-constexpr float kCapFactor[GX_NQ] = {6.f, 3.f, 3.f, 3.f, 3.f, 6.f, 3.f, 3.f, 3.f, 3.f,
-                                     6.f, 6.f, 3.f, 3.f, 6.f, 6.f, 3.f, 3.f};
+constexpr float kCapFactor[GX_NQ] = {6.f, 3.f, 3.f, 3.f, 3.f, 6.f, 3.f, 3.f, 3.f, 3.f,   // stages
+                                     2.f, 2.f, 2.f, 2.f, 3.f, 3.f,                        // photon continuations
+                                     2.f, 2.f, 2.f, 2.f, 3.f, 3.f};
 
 constexpr unsigned long long cap_factor_sum()
 {
@@ -25,7 +26,7 @@ constexpr unsigned long long cap_factor_sum()
 constexpr unsigned long long estate_factor_sum()
 {
     unsigned long long t = 0;
-    for (int q = GX_Q_ECONT; q < GX_Q_ECONT + 4; q++) t += (unsigned long long)kCapFactor[q];
+    for (int q = GX_Q_ECONT; q < GX_Q_ECONT + GX_NESTATE; q++) t += (unsigned long long)kCapFactor[q];
     return t;
 }
 
@@ -55,7 +56,7 @@ struct gegs_engine {
     uint32_t trace_cap = 0;
     uint32_t *d_qmeta = nullptr;       // count[GX_NQ], head[GX_NQ], done[GX_NQ]
     Part *d_qbuf[GX_NQ] = {};
-    EStatePk *d_estate[4] = {};
+    EStatePk *d_estate[GX_NESTATE] = {};
     uint32_t qcap[GX_NQ] = {};
     uint32_t batch = 0;
 
@@ -144,7 +145,7 @@ void gegs_destroy(gegs_engine *e)
     cudaFree(e->d_err); cudaFree(e->d_stats); cudaFree(e->d_sched); cudaFree(e->d_qmeta);
     cudaFree(e->d_trace); cudaFree(e->d_trace_n);
     for (int q = 0; q < GX_NQ; q++) cudaFree(e->d_qbuf[q]);
-    for (int k = 0; k < 4; k++) cudaFree(e->d_estate[k]);
+    for (int k = 0; k < GX_NESTATE; k++) cudaFree(e->d_estate[k]);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -298,7 +299,8 @@ static gegs_status ensure_queues(gegs_engine *e, uint32_t batch)
         CK(realloc_dev(&e->d_qbuf[q], (size_t)cap), "queue buffer");
         e->qcap[q] = (uint32_t)cap;
     }
-    for (int k = 0; k < 4; k++) CK(realloc_dev(&e->d_estate[k], (size_t)e->qcap[GX_Q_ECONT + k]), "electron state");
+    for (int k = 0; k < GX_NESTATE; k++)
+        CK(realloc_dev(&e->d_estate[k], (size_t)e->qcap[GX_Q_ECONT + k]), "electron state");
     e->batch = batch;
     e->ctx_gen++;
     return GEGS_OK;
@@ -308,7 +310,7 @@ static void fill_queue_ctx(gegs_engine *e)
 {
     QueueSet &Q = e->ctx.q;
     for (int q = 0; q < GX_NQ; q++) { Q.buf[q] = e->d_qbuf[q]; Q.cap[q] = e->qcap[q]; }
-    for (int k = 0; k < 4; k++) Q.estate[k] = e->d_estate[k];
+    for (int k = 0; k < GX_NESTATE; k++) Q.estate[k] = e->d_estate[k];
     Q.count = e->d_qmeta;
     Q.head = e->d_qmeta + GX_NQ;
     Q.done = e->d_qmeta + 2 * GX_NQ;
@@ -320,13 +322,15 @@ static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
     const DevCtx &C = e->ctx;
     cudaStream_t s = e->stream;
     k_source<<<grid, threads, 0, s>>>(C, e->d_sched);
-    k_photon_head<<<grid, threads, 0, s>>>(C);
+    k_photon_jaws<<<grid, threads, 0, s>>>(C);
+    k_photon_mlc<<<grid, threads, 0, s>>>(C);
     k_photon<<<grid, threads, 0, s>>>(C);
     k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(C);
     k_interact<ST_PHOTO><<<grid, threads, 0, s>>>(C);
     k_interact<ST_RAYLEIGH><<<grid, threads, 0, s>>>(C);
     k_interact<ST_PAIR><<<grid, threads, 0, s>>>(C);
-    k_electron_head<<<grid, threads, 0, s>>>(C);
+    k_electron_jaws<<<grid, threads, 0, s>>>(C);
+    k_electron_mlc<<<grid, threads, 0, s>>>(C);
     k_electron<<<grid, threads, 0, s>>>(C);
     k_interact<ST_MOLLER><<<grid, threads, 0, s>>>(C);
     k_interact<ST_BREMS><<<grid, threads, 0, s>>>(C);
@@ -398,7 +402,7 @@ extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hi
     CK(cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->stream), "err reset");
     CK(cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 16, e->stream), "stats reset");
 
-    for (int k = 0; k < 12; k++) { e->last.stage_ms[k] = 0.0; e->last.stage_launches[k] = 0; }
+    for (int k = 0; k < 16; k++) { e->last.stage_ms[k] = 0.0; e->last.stage_launches[k] = 0; }
     if (o.mode == GEGS_MODE_PERSISTENT) {
         st = build_graph(e, grid, threads);
         if (st != GEGS_OK) return st;
@@ -409,34 +413,35 @@ extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hi
     } else if (o.mode == GEGS_MODE_TIMED) {
         // Same kernels as the persistent graph, launched wave by wave with an
         // event pair around each launch to attribute device time per kernel.
-        for (int k = 0; k < 12; k++) { e->last.stage_ms[k] = 0.0; e->last.stage_launches[k] = 0; }
-        std::vector<cudaEvent_t> evs(28);
+        std::vector<cudaEvent_t> evs(32);
         for (auto &ev : evs) CK(cudaEventCreate(&ev), "event");
         CK(cudaEventRecord(e->ev0, e->stream), "event");
         SchedState hsr;
-        float acc[12] = {0};
-        unsigned long long nl[12] = {0};
+        float acc[16] = {0};
+        unsigned long long nl[16] = {0};
         for (uint32_t w = 0; w < max_waves; w++) {
-            CK(cudaEventRecord(evs[26], e->stream), "event");
+            CK(cudaEventRecord(evs[30], e->stream), "event");
             k_plan<<<1, 1, 0, e->stream>>>(e->ctx, e->d_sched);
-            CK(cudaEventRecord(evs[27], e->stream), "event");
+            CK(cudaEventRecord(evs[31], e->stream), "event");
             CK(cudaMemcpyAsync(&hsr, e->d_sched, sizeof hsr, cudaMemcpyDeviceToHost, e->stream), "sched D2H");
             CK(cudaStreamSynchronize(e->stream), "timed sync");
             float t = 0.0f;
-            cudaEventElapsedTime(&t, evs[26], evs[27]);
+            cudaEventElapsedTime(&t, evs[30], evs[31]);
             acc[11] += t; nl[11]++;
             if (!hsr.pending) break;
             const DevCtx &C = e->ctx;
             cudaStream_t s = e->stream;
-            // the head-class consumers (codes 20, 25) are booked to their particle's stage
-            int slot[13] = {10, 20, ST_PHOTON, ST_COMPTON, ST_PHOTO, ST_RAYLEIGH, ST_PAIR, 25, ST_ELECTRON, ST_MOLLER,
-                            ST_BREMS, ST_BHABHA, ST_ANNIH};
-            for (int k = 0; k < 13; k++) {
+            // codes 12 / 13: photon / electron consumers of the jaws, 14 / 15: of the MLC
+            int slot[15] = {10, 12, 14, ST_PHOTON, ST_COMPTON, ST_PHOTO, ST_RAYLEIGH, ST_PAIR, 13, 15, ST_ELECTRON,
+                            ST_MOLLER, ST_BREMS, ST_BHABHA, ST_ANNIH};
+            for (int k = 0; k < 15; k++) {
                 CK(cudaEventRecord(evs[2 * k], s), "event");
                 switch (slot[k]) {
                 case 10: k_source<<<grid, threads, 0, s>>>(C, e->d_sched); break;
-                case 20: k_photon_head<<<grid, threads, 0, s>>>(C); break;
-                case 25: k_electron_head<<<grid, threads, 0, s>>>(C); break;
+                case 12: k_photon_jaws<<<grid, threads, 0, s>>>(C); break;
+                case 13: k_electron_jaws<<<grid, threads, 0, s>>>(C); break;
+                case 14: k_photon_mlc<<<grid, threads, 0, s>>>(C); break;
+                case 15: k_electron_mlc<<<grid, threads, 0, s>>>(C); break;
                 case ST_PHOTON: k_photon<<<grid, threads, 0, s>>>(C); break;
                 case ST_COMPTON: k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(C); break;
                 case ST_PHOTO: k_interact<ST_PHOTO><<<grid, threads, 0, s>>>(C); break;
@@ -451,17 +456,16 @@ extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hi
                 CK(cudaEventRecord(evs[2 * k + 1], s), "event");
             }
             CK(cudaStreamSynchronize(s), "timed sync");
-            for (int k = 0; k < 13; k++) {
+            for (int k = 0; k < 15; k++) {
                 float tk = 0.0f;
                 cudaEventElapsedTime(&tk, evs[2 * k], evs[2 * k + 1]);
-                int kind = slot[k] >= 20 ? slot[k] - 20 : slot[k];
-                acc[kind] += tk;
-                nl[kind]++;
+                acc[slot[k]] += tk;
+                nl[slot[k]]++;
             }
         }
         CK(cudaEventRecord(e->ev1, e->stream), "event");
         for (auto &ev : evs) cudaEventDestroy(ev);
-        for (int k = 0; k < 12; k++) { e->last.stage_ms[k] = acc[k]; e->last.stage_launches[k] = nl[k]; }
+        for (int k = 0; k < 16; k++) { e->last.stage_ms[k] = acc[k]; e->last.stage_launches[k] = nl[k]; }
     } else {
         // Plain form: host-driven, one kernel per event type, synchronise and
         // read the queue counters back after every launch (CUDA_EGS.cu:226-365).
@@ -606,7 +610,7 @@ constexpr size_t kNoallocBytes =
     noalloc_align(sizeof(uint32_t) * 3 * GX_NQ) + noalloc_align(sizeof(SchedState)) +
     noalloc_align(sizeof(uint32_t)) + noalloc_align(sizeof(unsigned long long) * 16) +
     (cap_factor_sum() * GEGS_NOALLOC_MAX_BATCH + (size_t)GX_NQ * 4096u) * sizeof(Part) + (size_t)GX_NQ * 256u +
-    (estate_factor_sum() * GEGS_NOALLOC_MAX_BATCH + 4u * 4096u) * sizeof(EStatePk) + 4u * 256u;
+    (estate_factor_sum() * GEGS_NOALLOC_MAX_BATCH + GX_NESTATE * 4096u) * sizeof(EStatePk) + GX_NESTATE * 256u;
 
 constexpr int kNoallocMaxDevices = 64;
 
@@ -663,7 +667,8 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
         c.q.cap[q] = cap;
         c.q.buf[q] = (Part *)take((size_t)cap * sizeof(Part));
     }
-    for (int k = 0; k < 4; k++) c.q.estate[k] = (EStatePk *)take((size_t)c.q.cap[GX_Q_ECONT + k] * sizeof(EStatePk));
+    for (int k = 0; k < GX_NESTATE; k++)
+        c.q.estate[k] = (EStatePk *)take((size_t)c.q.cap[GX_Q_ECONT + k] * sizeof(EStatePk));
     if (off > kNoallocBytes) { e->err = "gegs_run_noalloc: scratch layout exceeds the array"; return GEGS_ERR_ARG; }
     c.q.count = qmeta;
     c.q.head = qmeta + GX_NQ;
@@ -695,13 +700,15 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
         for (int k = 0; k < 8 && w < hs.max_waves; k++, w++) {
             k_plan<<<1, 1, 0, s>>>(c, sched);
             k_source<<<grid, threads, 0, s>>>(c, sched);
-            k_photon_head<<<grid, threads, 0, s>>>(c);
+            k_photon_jaws<<<grid, threads, 0, s>>>(c);
+            k_photon_mlc<<<grid, threads, 0, s>>>(c);
             k_photon<<<grid, threads, 0, s>>>(c);
             k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(c);
             k_interact<ST_PHOTO><<<grid, threads, 0, s>>>(c);
             k_interact<ST_RAYLEIGH><<<grid, threads, 0, s>>>(c);
             k_interact<ST_PAIR><<<grid, threads, 0, s>>>(c);
-            k_electron_head<<<grid, threads, 0, s>>>(c);
+            k_electron_jaws<<<grid, threads, 0, s>>>(c);
+            k_electron_mlc<<<grid, threads, 0, s>>>(c);
             k_electron<<<grid, threads, 0, s>>>(c);
             k_interact<ST_MOLLER><<<grid, threads, 0, s>>>(c);
             k_interact<ST_BREMS><<<grid, threads, 0, s>>>(c);

@@ -46,7 +46,8 @@ __device__ __forceinline__ void consumer_done(const DevCtx &C, int q, int q2 = -
 __device__ __forceinline__ void push_cont(const DevCtx &C, int qid, Part p, const Rng &r, const EStatePk *st)
 {
     rng_store(r, p);
-    cg::coalesced_group g = cg::coalesced_threads();
+    // lanes of a warp may push to different queues here: one atomic per queue
+    cg::coalesced_group g = cg::labeled_partition(cg::coalesced_threads(), qid);
     uint32_t base = 0;
     if (g.thread_rank() == 0) base = atomicAdd(&C.q.count[qid], (uint32_t)g.size());
     base = g.shfl(base, 0);
@@ -199,26 +200,25 @@ __device__ __forceinline__ bool refill(const DevCtx &C, int hq, uint32_t n_cont,
 #endif
 
 // Transport consumer for photons (ELEC false) or electrons of one geometry
-// class G. The phantom-class kernel also takes the stage queue's new particles
-// (and hands those that start in the linac head to the head-class kernel);
-// the head-class kernel takes only its continuations. A particle outside the
-// class, or one whose step budget for this launch is spent, is re-queued for the
-// next wave with its state; the tally does not depend on where a track is split.
+// class G. The jaws kernel runs first in a wave and also takes the stage
+// queue's new particles. A particle outside the class is handed to its class's
+// continuation queue: that class's input of the same wave when its kernel runs
+// later in the wave (further along the beam), else of the next wave. A particle
+// whose step budget for this launch is spent is re-queued for the next wave.
+// Both carry the particle's state, so the tally does not depend on where a
+// track is split.
 template <bool ELEC, int G>
 __device__ __forceinline__ void transport_consumer(const DevCtx &C)
 {
     constexpr int Q = ELEC ? ST_ELECTRON : ST_PHOTON;
-    constexpr bool HEAD = (G == GX_GEOM_HEAD);
-    constexpr int own = ELEC ? (HEAD ? GX_Q_EHCONT : GX_Q_ECONT) : (HEAD ? GX_Q_PHCONT : GX_Q_PCONT);
-    constexpr int other = ELEC ? (HEAD ? GX_Q_ECONT : GX_Q_EHCONT) : (HEAD ? GX_Q_PCONT : GX_Q_PHCONT);
+    constexpr int base = ELEC ? GX_Q_ECONT : GX_Q_PCONT;
+    constexpr int cls = G - GX_GEOM_JAWS;                // 0 jaws, 1 MLC, 2 phantom
+    constexpr bool FIRST = (cls == 0);
     const uint32_t par = *C.wave & 1u;
-    // The head-class kernel runs first in a wave and hands particles to the
-    // phantom kernel of the same wave; the phantom kernel hands to the next wave.
-    const int qc_in = own + (int)par, qc_out = own + (int)(par ^ 1u);
-    const int qo_out = other + (int)(HEAD ? par : (par ^ 1u));
-    const int hq = HEAD ? qc_in : Q;
+    const int qc_in = base + 2 * cls + (int)par, qc_out = base + 2 * cls + (int)(par ^ 1u);
+    const int hq = FIRST ? Q : qc_in;
     const uint32_t n_cont = queue_len(C, qc_in);
-    const uint32_t n = n_cont + (HEAD ? 0u : queue_len(C, Q));
+    const uint32_t n = n_cont + (FIRST ? queue_len(C, Q) : 0u);
     const uint32_t budget = ELEC ? C.electron_budget : C.photon_budget;
     Part p;
     Rng r;
@@ -232,9 +232,11 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
         if (active && !was) nst = 0;
         if (!__any_sync(0xffffffffu, active)) break;
         if (active) {
-            if (G != GX_GEOM_ALL && !in_geom_class<G>(p)) {
-                if (ELEC) { EStatePk k = pack_estate(s); push_cont(C, qo_out, p, r, &k); }
-                else push_cont(C, qo_out, p, r, nullptr);
+            if (!in_geom_class<G>(p)) {
+                const int tc = geom_class_of(p.module) - GX_GEOM_JAWS;
+                const int tq = base + 2 * tc + (int)(tc > cls ? par : (par ^ 1u));
+                if (ELEC) { EStatePk k = pack_estate(s); push_cont(C, tq, p, r, &k); }
+                else push_cont(C, tq, p, r, nullptr);
                 active = false;
             } else {
                 steps++;
@@ -249,10 +251,20 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
             }
         }
     }
-    if (!HEAD) block_stat_add(C, Q, taken);
+    if (FIRST) block_stat_add(C, Q, taken);
     block_stat_add(C, GX_NSTAGE + (ELEC ? 1 : 0), steps);
-    if (HEAD) consumer_done(C, qc_in);
-    else consumer_done(C, Q, qc_in);
+    if (FIRST) consumer_done(C, Q, qc_in);
+    else consumer_done(C, qc_in);
+}
+
+__global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_jaws(const __grid_constant__ DevCtx C)
+{
+    transport_consumer<false, GX_GEOM_JAWS>(C);
+}
+
+__global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_mlc(const __grid_constant__ DevCtx C)
+{
+    transport_consumer<false, GX_GEOM_MLC>(C);
 }
 
 __global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon(const __grid_constant__ DevCtx C)
@@ -260,19 +272,19 @@ __global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon(const __gr
     transport_consumer<false, GX_GEOM_PHANTOM>(C);
 }
 
-__global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_head(const __grid_constant__ DevCtx C)
+__global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_jaws(const __grid_constant__ DevCtx C)
 {
-    transport_consumer<false, GX_GEOM_HEAD>(C);
+    transport_consumer<true, GX_GEOM_JAWS>(C);
+}
+
+__global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_mlc(const __grid_constant__ DevCtx C)
+{
+    transport_consumer<true, GX_GEOM_MLC>(C);
 }
 
 __global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron(const __grid_constant__ DevCtx C)
 {
     transport_consumer<true, GX_GEOM_PHANTOM>(C);
-}
-
-__global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_head(const __grid_constant__ DevCtx C)
-{
-    transport_consumer<true, GX_GEOM_HEAD>(C);
 }
 
 template <int Q>

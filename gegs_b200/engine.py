@@ -42,7 +42,7 @@ class RunOpts(C.Structure):
 class RunStats(C.Structure):
     _fields_ = [("processed", C.c_uint64 * 10), ("photon_steps", C.c_uint64), ("electron_steps", C.c_uint64),
                 ("waves", C.c_uint32), ("error_bits", C.c_uint32), ("device_ms", C.c_double),
-                ("stage_ms", C.c_double * 12), ("stage_launches", C.c_uint64 * 12)]
+                ("stage_ms", C.c_double * 16), ("stage_launches", C.c_uint64 * 16)]
 
 
 _lib = None

@@ -13,12 +13,13 @@ Windows separators are accepted, and a relative data directory is taken
 relative to the directory of the INI file.
 
 Supported sections: General, Data, Phase space, SecJaws, MLC, Phantom,
-Calibration, Output factor. The physics tables are built by this package's
+Calibration, Output factor, Interpolation, and the absolute (point) dose of
+[Dose output]. The physics tables are built by this package's
 table generator for the media the phantom and the beam line name (a PEGS4
 file named under [Data] is not read). Not supported, with a clear error when
-switched on: Block and Wedge modules, CTcreate from DICOM. Interpolation and
-the [Dose output] point/relative-dose and gamma comparisons against measured
-data are reported as skipped.
+switched on: Block and Wedge modules, CTcreate from DICOM. The [Dose output]
+relative-dose comparison against measured detector-array data is reported as
+skipped.
 """
 from __future__ import annotations
 
@@ -101,6 +102,7 @@ class Plan:
     dose_unit: float
     field_output_factors: list
     log: list = field(default_factory=list)
+    post: dict = field(default_factory=dict)      # interpolation grid, point-dose position
     nx: int = 0
     ny: int = 0
     nz: int = 0
@@ -209,11 +211,21 @@ def load_plan(ini_path, seed=SEED_BASE, max_histories=None) -> Plan:
     if _on(_get(ini, "Calibration", "dose calibration")):
         hpc = _floats(_get(ini, "Calibration", "histories per cGy", required=True), 1, "histories per cGy")[0]
         dose_unit = DOSE_UNIT * hpc / hpm
-    for sec, key in (("Interpolation", "do interpolate"), ("Dose output", "absolute dose"),
-                     ("Dose output", "relative dose")):
-        if _on(_get(ini, sec, key)):
-            log.append(f"[{sec}] {key} = Yes: not produced by this tool (dose grid only)")
+    post = {}
+    if _on(_get(ini, "Interpolation", "do interpolate")):
+        post["interp"] = dict(
+            start=_floats(_get(ini, "Interpolation", "starting point", required=True), 3, "starting point"),
+            dims=[int(v) for v in _floats(_get(ini, "Interpolation", "xyz dimensions", required=True), 3,
+                                          "xyz dimensions")],
+            sizes=_floats(_get(ini, "Interpolation", "3d voxel sizes", required=True), 3, "3d voxel sizes"))
+    if _on(_get(ini, "Dose output", "absolute dose")):
+        post["point"] = dict(
+            pos=_floats(_get(ini, "Dose output", "dose position", required=True), 3, "dose position"),
+            measured=_floats(_get(ini, "Dose output", "dose measured", "0"), 1, "dose measured")[0])
+    if _on(_get(ini, "Dose output", "relative dose")):
+        log.append("[Dose output] relative dose = Yes: the comparison with measured detector-array data is "
+                   "not produced by this tool")
     job = Job(f"plan {prefix}", media, phys, phantom, beam, fields, recs, h,
               meta=dict(seed=seed, mlc=mlc, jaws=jaws, ini=str(ini_path)))
     return Plan(job=job, prefix=prefix, output_dir=outdir, histories_per_mu=hpm, dose_unit=dose_unit,
-                field_output_factors=ofac, log=log, nx=ph["nx"], ny=ph["ny"], nz=ph["nz"])
+                field_output_factors=ofac, log=log, nx=ph["nx"], ny=ph["ny"], nz=ph["nz"], post=post)

@@ -1,0 +1,123 @@
+"""Dose post-processing and CT conversion through the CUDA library
+(include/gegs_post.h), plus the reference's scalar dose read-outs.
+
+* ``interp_dose``      dose on a regular output grid (interp_dose, output.c:221-316),
+  ``write_interp``     its file ``<base>_Interpolate_NNNxNNNxNNN.bin`` (3 x int32 dims + float32);
+* ``gamma3d``          3-D global gamma index and pass rate;
+* ``ct_ramp``          HU -> medium, density (CTToMedium's ramp, ctcreate.c:913-970);
+* ``point_dose``       the absolute dose at a point (output_AbsDos, output.c:780-871).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .engine import load_library
+
+_ready = False
+
+
+class CtRampSegment(C.Structure):
+    _fields_ = [("hu_upper", C.c_double), ("density_lower", C.c_double), ("density_upper", C.c_double),
+                ("medium", C.c_int32), ("pad_", C.c_int32)]
+
+
+def _lib():
+    global _ready
+    L = load_library()
+    if not _ready:
+        vp, f, i = C.c_void_p, C.c_float, C.c_int
+        L.gegs_interp_dose.argtypes = [i, vp, i, i, i, vp, vp, vp, f, f, f, f, f, f, i, i, i, vp]
+        L.gegs_gamma3d.argtypes = [i, vp, vp, i, i, i, f, f, f, f, f, f, f, vp, C.POINTER(C.c_uint64),
+                                   C.POINTER(C.c_uint64)]
+        L.gegs_ct_ramp.argtypes = [i, vp, C.c_uint64, vp, i, C.c_double, vp, vp]
+        _ready = True
+    return L
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"{what} failed with status {rc}")
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def interp_dose(dose, x_bounds, y_bounds, z_bounds, start, sizes, dims, device=0):
+    """dose: (nz, ny, nx) or flat, x fastest. Returns the (mz, my, mx) grid."""
+    nx, ny, nz = len(x_bounds) - 1, len(y_bounds) - 1, len(z_bounds) - 1
+    d = _f32(dose).reshape(-1)
+    xb, yb, zb = _f32(x_bounds), _f32(y_bounds), _f32(z_bounds)
+    mx, my, mz = (int(v) for v in dims)
+    out = np.empty(mx * my * mz, np.float32)
+    _check(_lib().gegs_interp_dose(device, d.ctypes.data, nx, ny, nz, xb.ctypes.data, yb.ctypes.data,
+                                   zb.ctypes.data, *(float(v) for v in start), *(float(v) for v in sizes),
+                                   mx, my, mz, out.ctypes.data), "gegs_interp_dose")
+    return out.reshape(mz, my, mx)
+
+
+def write_interp(base, grid):
+    mz, my, mx = grid.shape
+    name = f"{base}_Interpolate_{mx:03d}x{my:03d}x{mz:03d}.bin"
+    with open(name, "wb") as f:
+        f.write(np.array([mx, my, mz], np.int32).tobytes())
+        f.write(_f32(grid).tobytes())
+    return name
+
+
+def gamma3d(ref, ev, spacing, dta=0.1, dd=0.01, cutoff=0.10, search=3.0, device=0):
+    """Global gamma: dd and cutoff are fractions of max(ref), dta in cm, search
+    radius = search * dta. Returns (gamma array with -1 below the cutoff, pass rate)."""
+    r, e = _f32(ref), _f32(ev)
+    if r.shape != e.shape or r.ndim != 3:
+        raise ValueError("ref and eval must be (nz, ny, nx) arrays of one shape")
+    nz, ny, nx = r.shape
+    rmax = float(r.max())
+    g = np.empty(r.size, np.float32)
+    ne, npass = C.c_uint64(), C.c_uint64()
+    _check(_lib().gegs_gamma3d(device, r.ctypes.data, e.ctypes.data, nx, ny, nz, *(float(s) for s in spacing),
+                               float(dta), float(dd * rmax), float(cutoff * rmax), float(search), g.ctypes.data,
+                               C.byref(ne), C.byref(npass)), "gegs_gamma3d")
+    return g.reshape(r.shape), (npass.value / ne.value if ne.value else float("nan"))
+
+
+def ct_ramp(hu, segments, hu_lower, device=0):
+    """segments: (medium index, HU upper bound, density at the lower end, density at the upper end)."""
+    h = np.ascontiguousarray(hu, np.int16).reshape(-1)
+    seg = (CtRampSegment * len(segments))()
+    for k, (m, ub, dlo, dhi) in enumerate(segments):
+        seg[k] = CtRampSegment(float(ub), float(dlo), float(dhi), int(m), 0)
+    med = np.empty(h.size, np.uint16)
+    dens = np.empty(h.size, np.float32)
+    _check(_lib().gegs_ct_ramp(device, h.ctypes.data, h.size, C.cast(seg, C.c_void_p), len(segments),
+                               float(hu_lower), med.ctypes.data, dens.ctypes.data), "gegs_ct_ramp")
+    return med, dens
+
+
+def point_dose(dose, x_bounds, y_bounds, z_bounds, pos):
+    """Interpolated dose at `pos` between voxel centres, with the reference's
+    index search (output_AbsDos, output.c:780-871)."""
+    nx, ny, nz = len(x_bounds) - 1, len(y_bounds) - 1, len(z_bounds) - 1
+    d = _f32(dose).reshape(-1)
+    c = [((_f32(b)[:-1] + _f32(b)[1:]) / np.float32(2)).astype(np.float32) for b in (x_bounds, y_bounds, z_bounds)]
+    f = np.float32
+
+    def find(cb, n, v):
+        for i in range(1, n - 2):
+            if v > cb[i] and v <= cb[i + 1]:
+                return i
+        return 0 if v <= cb[1] else n - 2
+
+    px, py, pz = (f(v) for v in pos)
+    i, j, k = find(c[0], nx, px), find(c[1], ny, py), find(c[2], nz, pz)
+    xy = nx * ny
+    at = lambda a, b, cc: d[a + nx * b + xy * cc]
+    a0 = at(i, j, k) + (pz - c[2][k]) * (at(i, j, k + 1) - at(i, j, k)) / (c[2][k + 1] - c[2][k])
+    a1 = at(i + 1, j, k) + (pz - c[2][k]) * (at(i + 1, j, k + 1) - at(i + 1, j, k)) / (c[2][k + 1] - c[2][k])
+    a2 = at(i, j + 1, k) + (pz - c[2][k]) * (at(i, j + 1, k + 1) - at(i, j + 1, k)) / (c[2][k + 1] - c[2][k])
+    a3 = at(i + 1, j + 1, k) + (pz - c[2][k]) * (at(i + 1, j + 1, k + 1) - at(i + 1, j + 1, k)) / (c[2][k + 1] - c[2][k])
+    a0 = a0 + (py - c[1][j]) * (a2 - a0) / (c[1][j + 1] - c[1][j])
+    a1 = a1 + (py - c[1][j]) * (a3 - a1) / (c[1][j + 1] - c[1][j])
+    return float(a0 + (px - c[0][i]) * (a1 - a0) / (c[0][i + 1] - c[0][i]))

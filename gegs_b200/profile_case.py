@@ -29,7 +29,7 @@ def main():
     eng.set_scene(job.scene())
     st = eng.run(0, args.histories, mode=MODE_TIMED, batch=args.batch)
     kinds = ["photon", "compton", "photo", "rayleigh", "pair", "electron", "moller", "brems", "bhabha", "annih",
-             "source", "planner"]
+             "source", "planner", "photon_jaws", "electron_jaws", "photon_mlc", "electron_mlc"]
     print(json.dumps({
         "workload": f"C3 CT head {dims[0]}x{dims[1]}x{dims[2]}, 5 fields, timed wave form",
         "histories": args.histories, "batch": args.batch, "waves": st["waves"],

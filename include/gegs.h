@@ -54,7 +54,7 @@ typedef enum gegs_mode {
 
 typedef struct gegs_run_opts {
     int32_t mode;              /* gegs_mode */
-    uint32_t batch;            /* particles kept in flight (0 = default 4M; queue memory ~5.2 KB each) */
+    uint32_t batch;            /* particles kept in flight (0 = default 4M; queue memory ~4.4 KB each) */
     int32_t blocks_per_sm;     /* 0 = default */
     int32_t threads_per_block; /* 0 = default */
     uint32_t max_waves;        /* safety budget (0 = default) */
@@ -71,8 +71,10 @@ typedef struct gegs_run_stats {
     uint32_t waves;
     uint32_t error_bits;
     double device_ms;          /* device time of the last gegs_run (CUDA events) */
-    double stage_ms[12];       /* GEGS_MODE_TIMED: device ms per kernel kind (10 stages, source, planner) */
-    uint64_t stage_launches[12];
+    double stage_ms[16];       /* GEGS_MODE_TIMED: device ms per kernel kind: 10 stages (photon and electron
+                                  in the phantom), source, planner, photon and electron in the jaws,
+                                  photon and electron in the MLC */
+    uint64_t stage_launches[16];
 } gegs_run_stats;
 
 /* Engine life cycle */

@@ -13,8 +13,8 @@ ROOT = Path(__file__).resolve().parents[1]
 
 
 def declared_functions():
-    txt = (ROOT / "include" / "gegs.h").read_text()
-    return sorted(set(re.findall(r"\b(gegs_[a-z_]+)\s*\(", txt)))
+    txt = "".join(p.read_text() for p in sorted((ROOT / "include").glob("*.h")))
+    return sorted(set(re.findall(r"\b(gegs_[a-z0-9_]+)\s*\(", txt)))
 
 
 def test_library_exports_all_declared_symbols():

@@ -182,10 +182,29 @@ def test_dose_file_layout(tmp_path):
 def test_command_line_writes_the_dose_grid(tmp_path, oracle):
     from gegs_b200.__main__ import run_plan
     job = _job()
-    ini = _write_plan(tmp_path, job, extra="")
+    ini = _write_plan(tmp_path, job, extra="""
+[Interpolation]
+do interpolate = Yes
+starting point = -2.3 -2.3 -2.9
+xyz dimensions = 60 60 20
+3d voxel sizes = 0.08 0.08 0.3
+
+[Dose output]
+absolute dose = Yes
+dose position = 0.1 0.2 0.3
+dose measured = 0
+""")
     name = run_plan(str(ini))
     plan = load_plan(ini)
     ref, _ = oracle.run(plan.job.physics, plan.job.scene(), 0, plan.job.histories)
     want = (ref.astype(np.float64) * 2.0 ** -30 / plan.job.voxel_mass() * plan.dose_unit).astype(np.float32)
     np.testing.assert_array_equal(F.read_dose(name).reshape(-1), want)
-    assert (tmp_path / "out" / "T1_log.txt").exists()
+    log = (tmp_path / "out" / "T1_log.txt").read_text()
+    assert "absolute dose at" in log
+    from oracle.post_oracle import interp_dose as ref_interp
+    grid = np.fromfile(tmp_path / "out" / "T1_Interpolate_060x060x020.bin", np.float32)
+    assert grid[:3].view(np.int32).tolist() == [60, 60, 20]
+    p = plan.job.phantom
+    np.testing.assert_array_equal(grid[3:].reshape(20, 60, 60),
+                                  ref_interp(want, p["x_bounds"], p["y_bounds"], p["z_bounds"],
+                                             (-2.3, -2.3, -2.9), (0.08, 0.08, 0.3), (60, 60, 20)))
