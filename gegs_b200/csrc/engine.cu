@@ -37,6 +37,10 @@ struct gegs_engine {
     int nsm = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // side streams and events that fork the independent kernels of a wave into
+    // parallel branches of the persistent graph
+    cudaStream_t aux[3] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[3] = {};
     std::string err;
 
     gegs_physics *d_P = nullptr;
@@ -124,6 +128,11 @@ gegs_status gegs_create(int device, gegs_engine **out)
     CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "stream");
     CK(cudaEventCreate(&e->ev0), "event");
     CK(cudaEventCreate(&e->ev1), "event");
+    for (int k = 0; k < 3; k++) {
+        CK(cudaStreamCreateWithFlags(&e->aux[k], cudaStreamNonBlocking), "stream");
+        CK(cudaEventCreateWithFlags(&e->ev_join[k], cudaEventDisableTiming), "event");
+    }
+    CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming), "event");
     CK(cudaMalloc(&e->d_err, sizeof(uint32_t)), "err");
     CK(cudaMalloc(&e->d_stats, sizeof(unsigned long long) * 16), "stats");
     CK(cudaMalloc(&e->d_sched, sizeof(SchedState)), "sched");
@@ -148,6 +157,11 @@ void gegs_destroy(gegs_engine *e)
     for (int k = 0; k < GX_NESTATE; k++) cudaFree(e->d_estate[k]);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
+    for (int k = 0; k < 3; k++) {
+        if (e->aux[k]) cudaStreamDestroy(e->aux[k]);
+        if (e->ev_join[k]) cudaEventDestroy(e->ev_join[k]);
+    }
+    if (e->ev_fork) cudaEventDestroy(e->ev_fork);
     if (e->stream) cudaStreamDestroy(e->stream);
     delete e;
 }
@@ -317,25 +331,48 @@ static void fill_queue_ctx(gegs_engine *e)
     e->ctx.wave = &e->d_sched->waves;
 }
 
+// One wave of the persistent form, as captured into the graph body. Kernels
+// with no data between them run as parallel branches: the three photon
+// consumers, the four photon interactions, the three electron consumers and
+// the four electron interactions (each reads its own queues; the pushes they
+// share are atomic appends read only by a later phase).
 static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
 {
     const DevCtx &C = e->ctx;
-    cudaStream_t s = e->stream;
+    cudaStream_t s = e->stream, *a = e->aux;
+    auto fork = [&](int n) {
+        cudaEventRecord(e->ev_fork, s);
+        for (int k = 0; k < n; k++) cudaStreamWaitEvent(a[k], e->ev_fork, 0);
+    };
+    auto join = [&](int n) {
+        for (int k = 0; k < n; k++) {
+            cudaEventRecord(e->ev_join[k], a[k]);
+            cudaStreamWaitEvent(s, e->ev_join[k], 0);
+        }
+    };
     k_source<<<grid, threads, 0, s>>>(C, e->d_sched);
-    k_photon_jaws<<<grid, threads, 0, s>>>(C);
-    k_photon_mlc<<<grid, threads, 0, s>>>(C);
+    fork(2);
+    k_photon_jaws<<<grid, threads, 0, a[0]>>>(C);
+    k_photon_mlc<<<grid, threads, 0, a[1]>>>(C);
     k_photon<<<grid, threads, 0, s>>>(C);
+    join(2);
+    fork(3);
     k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(C);
-    k_interact<ST_PHOTO><<<grid, threads, 0, s>>>(C);
-    k_interact<ST_RAYLEIGH><<<grid, threads, 0, s>>>(C);
-    k_interact<ST_PAIR><<<grid, threads, 0, s>>>(C);
-    k_electron_jaws<<<grid, threads, 0, s>>>(C);
-    k_electron_mlc<<<grid, threads, 0, s>>>(C);
+    k_interact<ST_PHOTO><<<grid, threads, 0, a[0]>>>(C);
+    k_interact<ST_RAYLEIGH><<<grid, threads, 0, a[1]>>>(C);
+    k_interact<ST_PAIR><<<grid, threads, 0, a[2]>>>(C);
+    join(3);
+    fork(2);
+    k_electron_jaws<<<grid, threads, 0, a[0]>>>(C);
+    k_electron_mlc<<<grid, threads, 0, a[1]>>>(C);
     k_electron<<<grid, threads, 0, s>>>(C);
+    join(2);
+    fork(3);
     k_interact<ST_MOLLER><<<grid, threads, 0, s>>>(C);
-    k_interact<ST_BREMS><<<grid, threads, 0, s>>>(C);
-    k_interact<ST_BHABHA><<<grid, threads, 0, s>>>(C);
-    k_interact<ST_ANNIH><<<grid, threads, 0, s>>>(C);
+    k_interact<ST_BREMS><<<grid, threads, 0, a[0]>>>(C);
+    k_interact<ST_BHABHA><<<grid, threads, 0, a[1]>>>(C);
+    k_interact<ST_ANNIH><<<grid, threads, 0, a[2]>>>(C);
+    join(3);
 }
 
 static gegs_status build_graph(gegs_engine *e, int grid, int threads)

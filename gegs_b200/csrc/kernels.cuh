@@ -200,20 +200,18 @@ __device__ __forceinline__ bool refill(const DevCtx &C, int hq, uint32_t n_cont,
 #endif
 
 // Transport consumer for photons (ELEC false) or electrons of one geometry
-// class G. The jaws kernel runs first in a wave and also takes the stage
-// queue's new particles. A particle outside the class is handed to its class's
-// continuation queue: that class's input of the same wave when its kernel runs
-// later in the wave (further along the beam), else of the next wave. A particle
-// whose step budget for this launch is spent is re-queued for the next wave.
-// Both carry the particle's state, so the tally does not depend on where a
-// track is split.
+// class G. The three class kernels of a particle type run concurrently; the
+// phantom kernel also takes the stage queue's new particles. A particle
+// outside the class, or one whose step budget for this launch is spent, is
+// re-queued with its state for the next wave (into its class's continuation
+// queue), so the tally does not depend on where a track is split.
 template <bool ELEC, int G>
 __device__ __forceinline__ void transport_consumer(const DevCtx &C)
 {
     constexpr int Q = ELEC ? ST_ELECTRON : ST_PHOTON;
     constexpr int base = ELEC ? GX_Q_ECONT : GX_Q_PCONT;
     constexpr int cls = G - GX_GEOM_JAWS;                // 0 jaws, 1 MLC, 2 phantom
-    constexpr bool FIRST = (cls == 0);
+    constexpr bool FIRST = (G == GX_GEOM_PHANTOM);        // takes the new particles
     const uint32_t par = *C.wave & 1u;
     const int qc_in = base + 2 * cls + (int)par, qc_out = base + 2 * cls + (int)(par ^ 1u);
     const int hq = FIRST ? Q : qc_in;
@@ -233,8 +231,7 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
         if (!__any_sync(0xffffffffu, active)) break;
         if (active) {
             if (!in_geom_class<G>(p)) {
-                const int tc = geom_class_of(p.module) - GX_GEOM_JAWS;
-                const int tq = base + 2 * tc + (int)(tc > cls ? par : (par ^ 1u));
+                const int tq = base + 2 * (geom_class_of(p.module) - GX_GEOM_JAWS) + (int)(par ^ 1u);
                 if (ELEC) { EStatePk k = pack_estate(s); push_cont(C, tq, p, r, &k); }
                 else push_cont(C, tq, p, r, nullptr);
                 active = false;
