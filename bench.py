@@ -227,7 +227,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--plain-histories", type=int, default=2_000_000,
+    ap.add_argument("--plain-histories", type=int, default=10_000_000,
                     help="histories of the plain-form comparison (0: skip)")
     ap.add_argument("--c4-histories", type=int, default=50_000_000,
                     help="forward/backward histories of the C4 gradient measurement (0: skip)")
