@@ -417,7 +417,7 @@ extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hi
     int bps = o.blocks_per_sm ? o.blocks_per_sm : 4;
     int grid = e->nsm * bps;
     uint32_t max_waves = o.max_waves ? o.max_waves : 200000u;
-    uint32_t pb = (o.step_budget & 0xFFFFu) ? (o.step_budget & 0xFFFFu) : 16u;
+    uint32_t pb = (o.step_budget & 0xFFFFu) ? (o.step_budget & 0xFFFFu) : 32u;
     uint32_t eb = (o.step_budget >> 16) ? (o.step_budget >> 16) : 8u;
     if (pb != e->ctx.photon_budget || eb != e->ctx.electron_budget) {
         e->ctx.photon_budget = pb;
@@ -433,7 +433,7 @@ extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hi
     hs.end = hist_end;
     hs.batch = batch;
     hs.max_waves = max_waves;
-    hs.refill_below = o.refill_below ? o.refill_below : (batch / 50u > 0u ? batch / 50u : 1u);
+    hs.refill_below = o.refill_below ? o.refill_below : (batch / 4u > 0u ? batch / 4u : 1u);
     CK(cudaMemcpyAsync(e->d_sched, &hs, sizeof hs, cudaMemcpyHostToDevice, e->stream), "sched H2D");
     CK(cudaMemsetAsync(e->d_qmeta, 0, sizeof(uint32_t) * 3 * GX_NQ, e->stream), "qmeta reset");
     CK(cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->stream), "err reset");

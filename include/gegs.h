@@ -59,9 +59,9 @@ typedef struct gegs_run_opts {
     int32_t threads_per_block; /* 0 = default */
     uint32_t max_waves;        /* safety budget (0 = default) */
     uint32_t step_budget;      /* steps per particle per launch before it is continued in the next wave:
-                                  bits 0-15 photons, 16-31 electrons (0 = defaults 16 / 8) */
+                                  bits 0-15 photons, 16-31 electrons (0 = defaults 32 / 8) */
     uint32_t refill_below;     /* new histories are injected once fewer than this many particles are in
-                                  flight, topping the population up to `batch` (0 = default batch / 50) */
+                                  flight, topping the population up to `batch` (0 = default batch / 4) */
 } gegs_run_opts;
 
 typedef struct gegs_run_stats {
