@@ -498,9 +498,8 @@ __device__ void hownear_mlc(const DevCtx &C, Part &p, float &tperp)
         inside_XZ = point_in_polygon_local(p1, C.boundaryXZ, 4);
         inside_YZ = point_in_polygon_local(p2, C.boundaryYZ, 4);
     } else { inside_XZ = 1; inside_YZ = 1; }
-    float bxz = point_min_dist_to_polygon<true>(p1, C.boundaryXZ, 4);
-    float byz = point_min_dist_to_polygon<true>(p2, C.boundaryYZ, 4);
-    if (bxz < byz) bound = bxz; else bound = byz;
+    // the distance to the MLC boundary is needed only outside the MLC (the
+    // reference computes it first in every case; the result is the same)
     if (inside_XZ && inside_YZ) {
         if (p.leafIndex > GX_PASSMLC) index = p.leafIndex;
         else { index = index_of_leaf(C, p1); p.leafIndex = (int8_t)index; }
@@ -522,6 +521,9 @@ __device__ void hownear_mlc(const DevCtx &C, Part &p, float &tperp)
         }
         if (tperp_xz < tperp_yz) tperp = tperp_xz; else tperp = tperp_yz;
     } else {
+        float bxz = point_min_dist_to_polygon<true>(p1, C.boundaryXZ, 4);
+        float byz = point_min_dist_to_polygon<true>(p2, C.boundaryYZ, 4);
+        if (bxz < byz) bound = bxz; else bound = byz;
         tperp = bound;
     }
 }
