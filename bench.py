@@ -173,6 +173,29 @@ def c4_gradient(args, eng):
             "grad_norm": float(np.linalg.norm(g_full))}
 
 
+def c5_batch(args, device):
+    """C5 serving-style batch: independent plans of mixed size run concurrently
+    (one engine, stream and persistent graph per plan) and then one by one;
+    wall time of each (launch of every plan to the end of the last)."""
+    from gegs_b200 import workloads as W
+    from gegs_b200.batch import PlanBatch
+    jobs = W.config5(n_plans=args.c5_plans, hist_min=args.c5_hist_max // 100, hist_max=args.c5_hist_max,
+                     nphsp=1_000_000)
+    pb = PlanBatch(jobs, device=device, memory_budget_gb=40.0)
+    pb.run([max(1, j.histories // 100) for j in jobs])            # warm-up: graphs and queues
+    total = sum(j.histories for j in jobs)
+    pb.run()
+    conc = pb.wall_s
+    pb.run_sequential()
+    seq = pb.wall_s
+    pb.close()
+    return {"workload": f"C5: {len(jobs)} plans (slab and CT head, 16^3..256x256x128 voxels, 1-7 fields), "
+                        f"histories log-uniform {args.c5_hist_max // 100}..{args.c5_hist_max}",
+            "histories": total, "concurrent_s": conc, "sequential_s": seq,
+            "concurrent_histories_per_s": total / conc, "sequential_histories_per_s": total / seq,
+            "timing": "host wall clock from the first launch to the last wait"}
+
+
 def make_job(args, histories):
     from gegs_b200 import workloads as W
     return W.config3(histories=histories, nphsp=args.nphsp)
@@ -232,6 +255,8 @@ def main():
     ap.add_argument("--c4-histories", type=int, default=50_000_000,
                     help="forward/backward histories of the C4 gradient measurement (0: skip)")
     ap.add_argument("--c4-fd-histories", type=int, default=5_000_000)
+    ap.add_argument("--c5-plans", type=int, default=32, help="plans of the batched sweep (0: skip)")
+    ap.add_argument("--c5-hist-max", type=int, default=10_000_000)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -388,6 +413,7 @@ def main():
 
     # ---- C4: beamlet gradient by replay vs forward and finite differences ---
     grad = c4_gradient(args, eng) if args.c4_histories > 0 else None
+    batched = c5_batch(args, local) if args.c5_plans > 0 else None
 
     cpu = None
     if not args.no_cpu:
@@ -419,6 +445,7 @@ def main():
         "clocks": clk.summary(),
         "plain_form": plain,
         "gradient": grad,
+        "batched_plans": batched,
         "stat_uncertainty": {"mean_rel_se_above_50pct_dmax": sig, "batches": args.steps,
                              "voxels": "density >= 0.1 g/cm3 with batch-mean dose > 50 % of its maximum",
                              "time_to_1pct_s": t1pct},

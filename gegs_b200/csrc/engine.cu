@@ -82,6 +82,7 @@ struct gegs_engine {
     double *d_grad = nullptr;          // [GX_GRAD_COPIES][nbeamlets]
 
     gegs_run_stats last{};
+    bool in_flight = false;            // gegs_launch queued a run that gegs_wait has not finished
 };
 
 static gegs_status cuda_fail(gegs_engine *e, cudaError_t c, const char *what)
@@ -406,9 +407,15 @@ static gegs_status build_graph(gegs_engine *e, int grid, int threads)
     return GEGS_OK;
 }
 
-extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts)
+static gegs_status run_finish(gegs_engine *e);
+
+// The transport of a run; with launch_only (persistent form) it returns once
+// the graph is queued on the engine's stream, and run_finish completes it.
+static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts,
+                            bool launch_only)
 {
     if (!e || !e->have_scene || hist_end < hist_begin) return GEGS_ERR_ARG;
+    if (e->in_flight) { e->err = "a launched run has not been waited for (gegs_wait)"; return GEGS_ERR_ARG; }
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     gegs_run_opts o = {};
     if (opts) o = *opts;
@@ -538,6 +545,16 @@ extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hi
         CK(cudaEventRecord(e->ev1, e->stream), "event");
     }
     CK(cudaGetLastError(), "launch");
+    if (launch_only && o.mode == GEGS_MODE_PERSISTENT) {
+        e->in_flight = true;
+        return GEGS_OK;
+    }
+    return run_finish(e);
+}
+
+static gegs_status run_finish(gegs_engine *e)
+{
+    e->in_flight = false;
     CK(cudaStreamSynchronize(e->stream), "run sync");
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e->ev0, e->ev1);
@@ -559,6 +576,27 @@ extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hi
     if (errbits & GX_ERR_SOURCE) { e->err = "history outside every field range"; return GEGS_ERR_SOURCE; }
     if (errbits & GX_ERR_STEP_BUDGET) { e->err = "wave budget exhausted"; return GEGS_ERR_STEP_BUDGET; }
     return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts)
+{
+    return run_impl(e, hist_begin, hist_end, opts, false);
+}
+
+extern "C" gegs_status gegs_launch(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts)
+{
+    gegs_run_opts o = {};
+    if (opts) o = *opts;
+    o.mode = GEGS_MODE_PERSISTENT;
+    return run_impl(e, hist_begin, hist_end, &o, true);
+}
+
+extern "C" gegs_status gegs_wait(gegs_engine *e)
+{
+    if (!e) return GEGS_ERR_ARG;
+    if (!e->in_flight) { e->err = "gegs_wait: no launched run"; return GEGS_ERR_ARG; }
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    return run_finish(e);
 }
 
 extern "C" gegs_status gegs_get_tally(gegs_engine *e, int64_t *out, uint64_t nvox)

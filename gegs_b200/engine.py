@@ -20,7 +20,7 @@ MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 
 EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
            "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_get_dose", "gegs_get_stats",
-           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version"]
+           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version"]
 
 
 TRACE_DTYPE = np.dtype([("kind_stage", "<u4"), ("hist_lo", "<u4"), ("sid_lo", "<u4"), ("sid_hi", "<u4"),
@@ -65,6 +65,8 @@ def load_library(path=None):
     L.gegs_set_phsp.argtypes = [vp, vp, C.c_uint64]
     L.gegs_run.argtypes = [vp, C.c_uint64, C.c_uint64, C.POINTER(RunOpts)]
     L.gegs_run_noalloc.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint32]
+    L.gegs_launch.argtypes = [vp, C.c_uint64, C.c_uint64, C.POINTER(RunOpts)]
+    L.gegs_wait.argtypes = [vp]
     L.gegs_set_beamlet_weights.argtypes = [vp, vp, C.c_uint32]
     L.gegs_backward.argtypes = [vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint32, C.POINTER(RunOpts)]
     L.gegs_reset_tally.argtypes = [vp]
@@ -148,6 +150,17 @@ class Engine:
         o = RunOpts(mode, batch, blocks_per_sm, threads, max_waves, (photon_budget & 0xFFFF) | (electron_budget << 16),
                     refill_below)
         self._check(self.L.gegs_run(self.h, h0, h1, C.byref(o)))
+        return self.stats()
+
+    def launch(self, h0: int, h1: int, batch: int = 0, blocks_per_sm: int = 0, threads: int = 0,
+               photon_budget: int = 0, electron_budget: int = 0, refill_below: int = 0):
+        """Queue a persistent-form run and return at once (see wait())."""
+        o = RunOpts(MODE_PERSISTENT, batch, blocks_per_sm, threads, 0, (photon_budget & 0xFFFF) | (electron_budget << 16),
+                    refill_below)
+        self._check(self.L.gegs_launch(self.h, h0, h1, C.byref(o)))
+
+    def wait(self):
+        self._check(self.L.gegs_wait(self.h))
         return self.stats()
 
     def reset_tally(self):

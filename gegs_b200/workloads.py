@@ -297,4 +297,29 @@ def config4(histories=50_000_000, seed=SEED_BASE + 4, nphsp=10_000_000, dims=(25
     return job
 
 
-CONFIGS = {1: config1, 2: config2, 3: config3, 4: config4}
+def config5(n_plans=32, seed=SEED_BASE + 5, hist_min=1_000_000, hist_max=100_000_000, nphsp=1_000_000,
+            dims_min=64, dims_max=(256, 256, 128)):
+    """C5: independent plans of mixed size for a serving-style batch. Phantom
+    sizes from dims_min^3 to dims_max (log-uniform per axis), 1-7 fields,
+    log-uniform history counts in [hist_min, hist_max]; even plans are the
+    slab phantom, odd plans the synthetic CT head with a seeded MLC."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for k in range(n_plans):
+        h = int(np.exp(rng.uniform(np.log(hist_min), np.log(hist_max))))
+        d = [int(np.exp(rng.uniform(np.log(min(dims_min, m)), np.log(m)))) for m in dims_max]
+        if k % 2 == 0:
+            n = max(16, min(d))
+            job = config2(histories=h, seed=seed * 100 + k, nphsp=min(nphsp, h), n=n)
+            desc = f"slab {n}^3, 1 field"
+        else:
+            nf = int(rng.integers(1, 8))
+            angles = tuple(float(a) for a in np.linspace(0.0, 360.0, nf, endpoint=False))
+            job = config3(histories=h, seed=seed * 100 + k, nphsp=min(nphsp, h), dims=tuple(d), angles=angles)
+            desc = f"CT {d[0]}x{d[1]}x{d[2]}, {nf} fields"
+        job.name = f"C5 plan {k}: {desc}, {h} histories"
+        jobs.append(job)
+    return jobs
+
+
+CONFIGS = {1: config1, 2: config2, 3: config3, 4: config4, 5: config5}

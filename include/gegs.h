@@ -97,6 +97,15 @@ gegs_status gegs_set_phsp(gegs_engine *e, const gegs_phsp_record *recs, uint64_t
  * the int64 tally (MeV * 2^30 per voxel).  opts may be NULL. */
 gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts);
 
+/* gegs_run in two halves, for running several engines (plans) at once on one
+ * GPU (no counterpart in the reference, which runs fields one after another):
+ * gegs_launch queues the persistent-form run on the engine's stream and
+ * returns; gegs_wait blocks until it is done and reports like gegs_run. Each
+ * engine has its own stream, so runs launched on several engines overlap on
+ * the device. One launched run per engine at a time. */
+gegs_status gegs_launch(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts);
+gegs_status gegs_wait(gegs_engine *e);
+
 /* No counterpart in the reference: an addition of this library.
  *
  * gegs_run_noalloc transports histories [hist_begin, hist_end) like gegs_run
