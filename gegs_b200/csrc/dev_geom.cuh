@@ -224,6 +224,23 @@ __device__ int index_of_leaf(const DevCtx &C, float2 p)
     return index;
 }
 
+// (u >= 0 && u < 1) for u = fl(num / den), den != 0, deciding from num and
+// den without the division where the outcome is certain and dividing
+// otherwise, so the decision is always that of the rounded quotient:
+// with n = num * sign(den) and d = |den| (exact), fl(num / den) = fl(n / d);
+// n < -d * 1e-30 gives a negative quotient that does not round to zero; n >= d
+// a quotient >= 1; 0 <= n <= d * (1 - 2^-20) a quotient below 1 - 2^-21.
+__device__ __forceinline__ bool edge_param_in_unit(float num, float den)
+{
+    float n = den > 0.0f ? num : -num;
+    float d = fabsf(den);
+    if (n < -d * 1e-30f) return false;
+    if (n >= d) return false;
+    if (n >= 0.0f && n <= d * 0.99999904632568359375f) return true;
+    float u = num / den;
+    return (u >= 0) && (u < 1);
+}
+
 template <bool LOCAL>
 __device__ float ray_intersect_polygon(float2 p0, float2 v, const float2 *poly, int n, int &inside)
 {
@@ -237,8 +254,7 @@ __device__ float ray_intersect_polygon(float2 p0, float2 v, const float2 *poly, 
         float tmp1 = v.x * (b.y - a.y) - v.y * (b.x - a.x);
         if (tmp1 != 0) {
             // the edge parameter first: most edges fail it, and then the distance is not needed
-            float u = ((a.x - p0.x) * v.y - (a.y - p0.y) * v.x) / tmp1;
-            if ((u >= 0) && (u < 1)) {
+            if (edge_param_in_unit(((a.x - p0.x) * v.y - (a.y - p0.y) * v.x), tmp1)) {
                 float dist = ((b.x - a.x) * (p0.y - a.y) - (b.y - a.y) * (p0.x - a.x)) / tmp1;
                 if (dist >= 0) {
                     count++;
@@ -461,7 +477,13 @@ __device__ __forceinline__ float point_dist2_to_segment(float2 p, float2 v, floa
 {
     float l2 = dist2p(v, w);
     if (l2 == 0) return dist2p(p, v);
-    float t = ((p.x - v.x) * (w.x - v.x) + (p.y - v.y) * (w.y - v.y)) / l2;
+    float tn = (p.x - v.x) * (w.x - v.x) + (p.y - v.y) * (w.y - v.y);
+    // t = fl(tn / l2) with l2 > 0: certainly negative (and not rounded to zero)
+    // below -l2 * 1e-30, certainly above 1 beyond l2 * (1 + 2^-20); only the
+    // projection case needs the quotient itself
+    if (tn < -l2 * 1e-30f) return dist2p(p, v);
+    if (tn > l2 * 1.00000095367431640625f) return dist2p(p, w);
+    float t = tn / l2;
     if (t < 0) return dist2p(p, v);
     if (t > 1) return dist2p(p, w);
     float2 a = make_float2(v.x + t * (w.x - v.x), v.y + t * (w.y - v.y));

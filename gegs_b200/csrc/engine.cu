@@ -568,6 +568,12 @@ static gegs_status run_finish(gegs_engine *e)
     for (int q = 0; q < GX_NSTAGE; q++) R.processed[q] = stats[q];
     R.photon_steps = stats[GX_NSTAGE];
     R.electron_steps = stats[GX_NSTAGE + 1];
+    R.photon_steps_class[0] = stats[GX_NSTAGE + 2];
+    R.photon_steps_class[1] = stats[GX_NSTAGE + 3];
+    R.photon_steps_class[2] = R.photon_steps - stats[GX_NSTAGE + 2] - stats[GX_NSTAGE + 3];
+    R.electron_steps_class[0] = stats[GX_NSTAGE + 4];
+    R.electron_steps_class[1] = stats[GX_NSTAGE + 5];
+    R.electron_steps_class[2] = R.electron_steps - stats[GX_NSTAGE + 4] - stats[GX_NSTAGE + 5];
     R.waves = hsr.waves;
     R.error_bits = errbits;
     R.device_ms = ms;

@@ -250,6 +250,8 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     }
     if (FIRST) block_stat_add(C, Q, taken);
     block_stat_add(C, GX_NSTAGE + (ELEC ? 1 : 0), steps);
+    // steps in the jaws and the MLC (slots 12-15; the phantom's are the rest)
+    if (cls < 2) block_stat_add(C, GX_NSTAGE + 2 + 2 * (ELEC ? 1 : 0) + cls, steps);
     if (FIRST) consumer_done(C, Q, qc_in);
     else consumer_done(C, qc_in);
 }

@@ -42,7 +42,8 @@ class RunOpts(C.Structure):
 class RunStats(C.Structure):
     _fields_ = [("processed", C.c_uint64 * 10), ("photon_steps", C.c_uint64), ("electron_steps", C.c_uint64),
                 ("waves", C.c_uint32), ("error_bits", C.c_uint32), ("device_ms", C.c_double),
-                ("stage_ms", C.c_double * 16), ("stage_launches", C.c_uint64 * 16)]
+                ("stage_ms", C.c_double * 16), ("stage_launches", C.c_uint64 * 16),
+                ("photon_steps_class", C.c_uint64 * 3), ("electron_steps_class", C.c_uint64 * 3)]
 
 
 _lib = None
@@ -182,7 +183,8 @@ class Engine:
         self._check(self.L.gegs_get_stats(self.h, C.byref(s)))
         return dict(processed=list(s.processed), photon_steps=s.photon_steps, electron_steps=s.electron_steps,
                     waves=s.waves, error_bits=s.error_bits, device_ms=s.device_ms,
-                    stage_ms=list(s.stage_ms), stage_launches=list(s.stage_launches))
+                    stage_ms=list(s.stage_ms), stage_launches=list(s.stage_launches),
+                    photon_steps_class=list(s.photon_steps_class), electron_steps_class=list(s.electron_steps_class))
 
     def set_trace(self, capacity: int):
         self._check(self.L.gegs_set_trace(self.h, capacity))

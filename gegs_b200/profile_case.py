@@ -34,6 +34,8 @@ def main():
         "workload": f"C3 CT head {dims[0]}x{dims[1]}x{dims[2]}, 5 fields, timed wave form",
         "histories": args.histories, "batch": args.batch, "waves": st["waves"],
         "photon_steps": st["photon_steps"], "electron_steps": st["electron_steps"],
+        "photon_steps_jaws_mlc_phantom": st["photon_steps_class"],
+        "electron_steps_jaws_mlc_phantom": st["electron_steps_class"],
         "processed": dict(zip(kinds[:10], st["processed"])),
         "stage_ms": dict(zip(kinds, st["stage_ms"])), "stage_launches": dict(zip(kinds, st["stage_launches"])),
         "error_bits": st["error_bits"]}))

@@ -75,6 +75,8 @@ typedef struct gegs_run_stats {
                                   in the phantom), source, planner, photon and electron in the jaws,
                                   photon and electron in the MLC */
     uint64_t stage_launches[16];
+    uint64_t photon_steps_class[3];   /* steps in the jaws, the MLC, the phantom (persistent and timed forms) */
+    uint64_t electron_steps_class[3];
 } gegs_run_stats;
 
 /* Engine life cycle */
