@@ -32,4 +32,10 @@ uint32_t ora_trace_count(void);
 int ora_run(const gegs_physics *P, const gegs_scene *S, uint64_t h0, uint64_t h1, int nthreads,
             int64_t *tally, ora_stats *stats);
 
+/* Known-answer probes (ora_probe.c). */
+int ora_probe_compton(const gegs_physics *P, int medium, uint32_t flags, float energy, uint32_t n, uint64_t seed,
+                      float *e_out, float *cos_out);
+void ora_probe_rotate(uint32_t n, uint64_t seed, float *norm_err, float *cos_err);
+uint32_t ora_probe_walk(const gegs_physics *P, const gegs_scene *S, int field, uint32_t region, const float pos[3],
+                        const float dir[3], uint32_t maxn, uint32_t *regions, float *steps);
 #endif

@@ -24,7 +24,7 @@ class Stats(C.Structure):
 
 
 def build(force=False):
-    srcs = list(HERE.glob("*.c")) + list(HERE.glob("*.h"))
+    srcs = list(HERE.glob("*.c")) + list(HERE.glob("*.h")) + list((HERE.parent / "include").glob("*.h"))
     if force or not LIB.exists() or any(s.stat().st_mtime > LIB.stat().st_mtime for s in srcs):
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
@@ -87,3 +87,41 @@ def run(physics: np.ndarray, scene_holder, h0: int, h1: int, threads: int = 0):
                  e_escaped=st.e_escaped, error=st.error, rc=rc,
                  cnt=[list(st.cnt[i]) for i in range(10)])
     return tally, stats
+
+
+# ---- known-answer probes (ora_probe.c) ------------------------------------
+def probe_compton(physics, medium, flags, energy, n, seed=1):
+    """Scattered-photon energy and cosine of n Compton events at `energy` (MeV)."""
+    L = lib()
+    blk = np.ascontiguousarray(physics)
+    e = np.zeros(n, np.float32)
+    c = np.zeros(n, np.float32)
+    L.ora_probe_compton.argtypes = [C.c_void_p, C.c_int, C.c_uint32, C.c_float, C.c_uint32, C.c_uint64,
+                                    C.c_void_p, C.c_void_p]
+    err = L.ora_probe_compton(blk.ctypes.data, medium, flags, energy, n, seed, e.ctypes.data, c.ctypes.data)
+    return e, c, err
+
+
+def probe_rotate(n, seed=1):
+    L = lib()
+    a = np.zeros(n, np.float32)
+    b = np.zeros(n, np.float32)
+    L.ora_probe_rotate.argtypes = [C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p]
+    L.ora_probe_rotate(n, seed, a.ctypes.data, b.ctypes.data)
+    return a, b
+
+
+def probe_walk(physics, scene_holder, pos, direction, field=0, region=1, maxn=4096):
+    """Regions entered and step lengths of howfar_phantom along one straight ray (beam frame)."""
+    L = lib()
+    blk = np.ascontiguousarray(physics)
+    regs = np.zeros(maxn, np.uint32)
+    steps = np.zeros(maxn, np.float32)
+    p = np.asarray(pos, np.float32)
+    d = np.asarray(direction, np.float32)
+    L.ora_probe_walk.restype = C.c_uint32
+    L.ora_probe_walk.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
+                                 C.c_void_p, C.c_void_p]
+    k = L.ora_probe_walk(blk.ctypes.data, C.addressof(scene_holder.scene), field, region, p.ctypes.data,
+                         d.ctypes.data, maxn, regs.ctypes.data, steps.ctypes.data)
+    return regs[:k], steps[:k]
