@@ -239,7 +239,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gegs", choices=["gegs", "reference"])
-    ap.add_argument("--hist-per-step", type=int, default=10_000_000)
+    ap.add_argument("--hist-per-step", type=int, default=40_000_000)
     ap.add_argument("--nphsp", type=int, default=10_000_000)
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--mode", default="persistent", choices=["persistent", "plain", "timed"],

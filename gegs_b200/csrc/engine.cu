@@ -419,13 +419,13 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     gegs_run_opts o = {};
     if (opts) o = *opts;
-    uint32_t batch = o.batch ? o.batch : (1u << 22);
+    uint32_t batch = o.batch ? o.batch : (3u << 21);
     int threads = o.threads_per_block ? o.threads_per_block : 256;
     int bps = o.blocks_per_sm ? o.blocks_per_sm : 4;
     int grid = e->nsm * bps;
     uint32_t max_waves = o.max_waves ? o.max_waves : 200000u;
     uint32_t pb = (o.step_budget & 0xFFFFu) ? (o.step_budget & 0xFFFFu) : 32u;
-    uint32_t eb = (o.step_budget >> 16) ? (o.step_budget >> 16) : 8u;
+    uint32_t eb = (o.step_budget >> 16) ? (o.step_budget >> 16) : 4u;
     if (pb != e->ctx.photon_budget || eb != e->ctx.electron_budget) {
         e->ctx.photon_budget = pb;
         e->ctx.electron_budget = eb;

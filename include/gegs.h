@@ -54,12 +54,13 @@ typedef enum gegs_mode {
 
 typedef struct gegs_run_opts {
     int32_t mode;              /* gegs_mode */
-    uint32_t batch;            /* particles kept in flight (0 = default 4M; queue memory ~4.4 KB each) */
+    uint32_t batch;            /* particles kept in flight (0 = default 6M = 3 << 21; queue memory ~4.4 KB each, ~28 GB at the default) */
     int32_t blocks_per_sm;     /* 0 = default */
     int32_t threads_per_block; /* 0 = default */
     uint32_t max_waves;        /* safety budget (0 = default) */
     uint32_t step_budget;      /* steps per particle per launch before it is continued in the next wave:
-                                  bits 0-15 photons, 16-31 electrons (0 = defaults 32 / 8) */
+                                  bits 0-15 photons, 16-31 electrons (0 = defaults 32 / 4); photons get
+                                  8x theirs in the jaws and MLC, electrons 2x theirs in the phantom */
     uint32_t refill_below;     /* new histories are injected once fewer than this many particles are in
                                   flight, topping the population up to `batch` (0 = default batch / 4) */
 } gegs_run_opts;
