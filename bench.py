@@ -161,6 +161,13 @@ def c4_gradient(args, eng):
     loss(beamlet_dose(w, small)).backward()
     g = w.grad.numpy()
     pick = np.argsort(-np.abs(g))[[0, 10, 100, 400]]
+    # 20 projected gradient-descent iterations (forward + replay backward each) on the small model
+    from gegs_b200.differentiable import optimize_weights
+    import time as _t
+    t0 = _t.perf_counter()
+    _, hist = optimize_weights(small, w0, target, organ, iterations=args.c4_iterations)
+    descent = {"iterations": args.c4_iterations, "histories_per_iteration": args.c4_fd_histories,
+               "objective_first": hist[0], "objective_last": hist[-1], "wall_s": _t.perf_counter() - t0}
     fd = fd_gradient(small, w0, pick, loss, delta=0.05)
     f_ms, b_ms = min(fwd), min(bwd)
     return {"workload": f"C4 CT head 256x256x120, 5 fields x 20x20 beamlets of 5 mm, {job.histories} histories",
@@ -170,7 +177,8 @@ def c4_gradient(args, eng):
             "fd_check": {"histories": args.c4_fd_histories, "beamlets": [int(b) for b in pick],
                          "replay": [float(x) for x in g[pick]], "fd": [float(x) for x in fd],
                          "max_rel_err": float(np.max(np.abs(g[pick] - fd) / np.abs(fd).max()))},
-            "grad_norm": float(np.linalg.norm(g_full))}
+            "grad_norm": float(np.linalg.norm(g_full)),
+            "descent": descent}
 
 
 def c5_batch(args, device):
@@ -255,6 +263,7 @@ def main():
     ap.add_argument("--c4-histories", type=int, default=50_000_000,
                     help="forward/backward histories of the C4 gradient measurement (0: skip)")
     ap.add_argument("--c4-fd-histories", type=int, default=5_000_000)
+    ap.add_argument("--c4-iterations", type=int, default=20)
     ap.add_argument("--c5-plans", type=int, default=32, help="plans of the batched sweep (0: skip)")
     ap.add_argument("--c5-hist-max", type=int, default=10_000_000)
     args = ap.parse_args()

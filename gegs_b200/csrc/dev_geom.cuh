@@ -525,21 +525,29 @@ __device__ void hownear_mlc(const DevCtx &C, Part &p, float &tperp)
     if (inside_XZ && inside_YZ) {
         if (p.leafIndex > GX_PASSMLC) index = p.leafIndex;
         else { index = index_of_leaf(C, p1); p.leafIndex = (int8_t)index; }
-        if (index >= 0) {
-            tperp_xz = point_min_dist_to_polygon<false>(p1, C.crossXZ + index * 16, 14);
-            const float2 *endn = endnode_of(C, p.field, index);
-            if (p.bank < 0) p.bank = (int8_t)point_in_leaf(p2, endn);
-            const float2 *yzp = endn;
-            int nv = 17;
-            if (p.bank == 0) { yzp += 2; nv = 30; }
-            else if (p.bank == 2) { yzp += 17; }
-            tperp_yz = point_min_dist_to_polygon<false>(p2, yzp, nv);
-        } else if (index > -60) {
-            int i = -index;
-            float t1 = point_min_dist_to_polygon<false>(p1, C.crossXZ + i * 16, 14);
-            i--;
-            tperp_xz = point_min_dist_to_polygon<false>(p1, C.crossXZ + i * 16, 14);
-            if (t1 < tperp_xz) tperp_xz = t1;
+        // In a leaf column: the leaf's XZ cross section, then its YZ leaf-end
+        // outline; in an air gap: the XZ cross sections of the two leaves on
+        // either side. Two polygon distances either way, taken in one loop so
+        // that lanes of both cases share it (each lane keeps the reference's
+        // polygons and order).
+        if (index >= 0 && p.bank < 0) p.bank = (int8_t)point_in_leaf(p2, endnode_of(C, p.field, index));
+        if (index > -60) {
+            const bool leaf = index >= 0;
+            const float2 *yzp = nullptr;
+            int nvyz = 17;
+            if (leaf) {
+                yzp = endnode_of(C, p.field, index);
+                if (p.bank == 0) { yzp += 2; nvyz = 30; }
+                else if (p.bank == 2) { yzp += 17; }
+            }
+            float dd[2];
+            for (int k = 0; k < 2; k++) {
+                const bool yz = leaf && k == 1;
+                const float2 *poly = leaf ? (k == 0 ? C.crossXZ + index * 16 : yzp) : C.crossXZ + (-index - k) * 16;
+                dd[k] = point_min_dist_to_polygon<false>(yz ? p2 : p1, poly, yz ? nvyz : 14);
+            }
+            if (leaf) { tperp_xz = dd[0]; tperp_yz = dd[1]; }
+            else tperp_xz = dd[0] < dd[1] ? dd[0] : dd[1];
         }
         if (tperp_xz < tperp_yz) tperp = tperp_xz; else tperp = tperp_yz;
     } else {

@@ -112,3 +112,23 @@ def beamlet_doses(model: BeamletModel, beamlets):
         w[b] = 1.0
         out.append(model.dose(w) - base)
     return out
+
+
+def optimize_weights(model: BeamletModel, w0, target, organ, iterations=20, lr=0.05, prescription=60.0,
+                     limit=20.0):
+    """Projected gradient descent on the beamlet weights (kept >= 0): each
+    iteration is one forward transport and one replay backward. Returns the
+    final weights and the objective per iteration."""
+    w = torch.tensor(np.asarray(w0, np.float64), requires_grad=True)
+    history = []
+    for _ in range(iterations):
+        w.grad = None
+        loss = objective(beamlet_dose(w, model), target, organ, prescription, limit)
+        loss.backward()
+        history.append(float(loss))
+        with torch.no_grad():
+            g = w.grad
+            step = lr * float(w.abs().mean()) / max(float(g.abs().max()), 1e-30)
+            w -= step * g
+            w.clamp_(min=0.0)
+    return w.detach().numpy(), history

@@ -75,3 +75,17 @@ def test_replay_gradient_matches_beamlet_doses_and_finite_differences(engine):
     # central differences, common random numbers
     fd = fd_gradient(model, w0, pick, loss, delta=0.05)
     np.testing.assert_allclose(g[pick], fd, rtol=2e-3, atol=2e-3 * np.abs(g[pick]).max())
+
+
+@pytest.mark.gpu
+def test_gradient_descent_lowers_the_objective(engine):
+    from gegs_b200.differentiable import BeamletModel, optimize_weights
+    job = _job(6000)
+    engine.set_physics(job.physics)
+    engine.set_scene(job.scene())
+    model = BeamletModel(engine, job)
+    w0 = job.beam["beamlets"]["weights"].astype(np.float64)
+    model.calibrate(w0, job.meta["target"], 50.0)
+    w, hist = optimize_weights(model, w0, job.meta["target"], job.meta["organ"], iterations=8)
+    assert len(hist) == 8 and hist[-1] < hist[0]
+    assert (w >= 0).all()
