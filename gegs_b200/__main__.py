@@ -63,6 +63,21 @@ def run_plan(ini, device=0, max_histories=None, out=sys.stdout):
         if pt["measured"]:
             msg += f" (measured {pt['measured']:.4g}, ratio {v / pt['measured']:.4f})"
         extra.append(msg)
+    if "relative" in plan.post:
+        from .postprocess import point_dose, read_measured, relative_dose, write_relative_dose
+        rp = plan.post["relative"]
+        if list(rp["dims"]) == [1, 1, 1]:          # one point: the reference reports the point dose instead
+            v = point_dose(dose.astype(np.float32), *bounds, rp["start"])
+            extra.append(f"absolute dose at ({rp['start'][0]:.2f}, {rp['start'][1]:.2f}, {rp['start'][2]:.2f})"
+                         f" = {v:.4g}")
+        else:
+            n = int(np.prod(rp["dims"]))
+            meas = read_measured(rp["measured"], n) if Path(rp["measured"]).is_file() else None
+            rl, tot, ok = relative_dose(dose.astype(np.float32), *bounds, rp["start"], rp["sizes"], rp["dims"],
+                                        meas, rp["norm_type"], rp["array_type"], rp["gamma_len_cm"],
+                                        rp["gamma_dos"], rp["iso"])
+            extra.append(f"relative dose {write_relative_dose(plan.output_base, rl, rp['dims'])}: "
+                         + (rl[-1] if meas is not None else f"measured data {rp['measured']} not readable"))
     lines = [f"plan {ini}", f"fields {len(job.fields)}, histories {job.histories}, phase-space particles {len(job.phsp)}",
              f"media {job.media}", f"dose unit {plan.dose_unit:.4e}",
              f"transport {wall:.3f} s ({job.histories / max(wall, 1e-9):.4g} histories/s), waves {st['waves']}",

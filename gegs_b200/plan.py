@@ -13,13 +13,11 @@ Windows separators are accepted, and a relative data directory is taken
 relative to the directory of the INI file.
 
 Supported sections: General, Data, Phase space, SecJaws, MLC, Phantom,
-Calibration, Output factor, Interpolation, and the absolute (point) dose of
-[Dose output]. The physics tables are built by this package's
+Calibration, Output factor, Interpolation, and [Dose output] (point dose and
+the relative-dose comparison with measured detector-array data). The physics tables are built by this package's
 table generator for the media the phantom and the beam line name (a PEGS4
 file named under [Data] is not read). Not supported, with a clear error when
-switched on: Block and Wedge modules, CTcreate from DICOM. The [Dose output]
-relative-dose comparison against measured detector-array data is reported as
-skipped.
+switched on: Block and Wedge modules, CTcreate from DICOM.
 """
 from __future__ import annotations
 
@@ -223,8 +221,18 @@ def load_plan(ini_path, seed=SEED_BASE, max_histories=None) -> Plan:
             pos=_floats(_get(ini, "Dose output", "dose position", required=True), 3, "dose position"),
             measured=_floats(_get(ini, "Dose output", "dose measured", "0"), 1, "dose measured")[0])
     if _on(_get(ini, "Dose output", "relative dose")):
-        log.append("[Dose output] relative dose = Yes: the comparison with measured detector-array data is "
-                   "not produced by this tool")
+        start = _floats(_get(ini, "Dose output", "starting point", required=True), 3, "starting point")
+        arr = (_get(ini, "Dose output", "PTW729/PTW1000", "") or "").strip()
+        norm = (_get(ini, "Dose output", "norm to Max/Center", "") or "").strip()
+        gl, gd = _floats(_get(ini, "Dose output", "gamma index (mm,%)", required=True), 2, "gamma index (mm,%)")
+        meas = _get(ini, "Dose output", "measured data", required=True)
+        post["relative"] = dict(
+            start=[start[k] + iso[k] for k in range(3)],
+            dims=[int(v) for v in _floats(_get(ini, "Dose output", "xyz dimensions", required=True), 3,
+                                          "xyz dimensions")],
+            sizes=_floats(_get(ini, "Dose output", "3d voxel sizes", required=True), 3, "3d voxel sizes"),
+            array_type=1 if arr == "PTW729" else 2, norm_type=1 if norm == "Max" else (2 if norm == "Center" else 0),
+            gamma_len_cm=float(np.float32(gl) * np.float32(0.1)), gamma_dos=float(np.float32(gd) * np.float32(0.01)), measured=data(meas), iso=list(iso))
     job = Job(f"plan {prefix}", media, phys, phantom, beam, fields, recs, h,
               meta=dict(seed=seed, mlc=mlc, jaws=jaws, ini=str(ini_path)))
     return Plan(job=job, prefix=prefix, output_dir=outdir, histories_per_mu=hpm, dose_unit=dose_unit,

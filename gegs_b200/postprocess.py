@@ -10,6 +10,7 @@
 from __future__ import annotations
 
 import ctypes as C
+from pathlib import Path
 
 import numpy as np
 
@@ -121,3 +122,128 @@ def point_dose(dose, x_bounds, y_bounds, z_bounds, pos):
     a0 = a0 + (py - c[1][j]) * (a2 - a0) / (c[1][j + 1] - c[1][j])
     a1 = a1 + (py - c[1][j]) * (a3 - a1) / (c[1][j + 1] - c[1][j])
     return float(a0 + (px - c[0][i]) * (a1 - a0) / (c[0][i + 1] - c[0][i]))
+
+
+def sample_plane(dose, x_bounds, y_bounds, z_bounds, start, sizes, dims):
+    """The dose of the voxel nearest each point of a comparison grid: the
+    reference's index `int((pos - c0) / (c1 - c0) + 0.1)` on voxel centres
+    (output_RelDos_II, output.c:606-624), the + 0.1 in double as in C."""
+    f = np.float32
+    d = _f32(dose).reshape(-1)
+    nx, ny, nz = len(x_bounds) - 1, len(y_bounds) - 1, len(z_bounds) - 1
+    c = [((_f32(b)[:-1] + _f32(b)[1:]) / f(2)).astype(np.float32) for b in (x_bounds, y_bounds, z_bounds)]
+    mx, my, mz = (int(v) for v in dims)
+    sx, sy, sz = (f(v) for v in sizes)
+    x0, y0, z0 = (f(v) for v in start)
+    calc = np.empty(mx * my * mz, np.float32)
+    for k in range(mz):
+        for j in range(my):
+            for i in range(mx):
+                px, py, pz = f(x0 + f(sx * f(i))), f(y0 + f(sy * f(j))), f(z0 + f(sz * f(k)))
+                ix = int(float(f((px - c[0][0]) / f(c[0][1] - c[0][0]))) + 0.1)    # + 0.1 in double
+                iy = int(float(f((py - c[1][0]) / f(c[1][1] - c[1][0]))) + 0.1)
+                iz = int(float(f((pz - c[2][0]) / f(c[2][1] - c[2][0]))) + 0.1)
+                calc[mx * my * k + mx * j + i] = d[nx * ny * iz + nx * iy + ix]
+    return calc
+
+
+def relative_dose(dose, x_bounds, y_bounds, z_bounds, start, sizes, dims, measured=None, norm_type=0,
+                  array_type=2, gamma_len_cm=0.3, gamma_dos=0.03, iso=(0.0, 0.0, 0.0)):
+    """The reference's comparison of the dose with detector-array data
+    (output_RelDos_II, output.c:596-778), in float32 as it computes it.
+
+    Samples the dose at the voxel nearest each point of the plane (start
+    already moved by the isocentre), normalises both to their maximum
+    (norm_type 1) or to the point at the isocentre (2), and marks each point
+    above 10 % of the measured maximum as passing when the dose difference is
+    within gamma_dos, or -- for the 1000-chamber array (array_type 2) -- when a
+    neighbouring point of the plane within gamma_len_cm agrees.
+    Without measured data the file lists the sampled doses alone.
+    Returns (lines of the result file, compared, passed)."""
+    f = np.float32
+    mx, my, mz = (int(v) for v in dims)
+    sx, sy, sz = (f(v) for v in sizes)
+    x0, y0, z0 = (f(v) for v in start)
+    calc = sample_plane(dose, x_bounds, y_bounds, z_bounds, start, sizes, dims)
+    if measured is None:
+        return [f"{v:f}" for v in calc], 0, 0
+    meas = _f32(measured).reshape(-1)[:calc.size].copy()
+    top = lambda a: max(f(0.0), a.max())  # the reference's running maxima start at 0
+    if norm_type == 1:
+        meas = meas / top(meas)
+        calc = calc / top(calc)
+        meas_max = f(1.0)
+    elif norm_type == 2:
+        center = 0
+        if sx != 0:
+            center += int(float(f(f(f(iso[0]) - x0) / sx)) + 0.1)
+        if sy != 0:
+            center += int(float(f(f(f(iso[1]) - y0) / sy)) + 0.1) * mx
+        if sz != 0:
+            center += int(float(f(f(f(iso[2]) - z0) / sz)) + 0.1) * mx * my
+        mc, cc = meas[center], calc[center]
+        meas_max = f(top(meas) / mc)
+        meas = meas / mc
+        calc = calc / cc
+    else:
+        meas = meas * f(100.0)
+        meas_max = top(meas)
+    thr = f(meas_max * f(0.1))
+    lines, total, count = [], 0, 0
+    dos, ln = f(gamma_dos), f(gamma_len_cm)
+    def near(a, m):                       # float ratio, squared in float; the sum and sqrt in double
+        v = f(f(f(abs(f(a - m)) / m) / dos))
+        v = f(v * v)
+        return f(np.sqrt(float(v) + 0.25 * 0.25 / float(ln) / float(ln)))
+    for i in range(calc.size):
+        pas = 0
+        m = meas[i]
+        if m > thr:
+            total += 1
+            if array_type == 1:
+                pas = 1 if f(abs(f(calc[i] - m)) / m) <= dos else -1
+                count += pas > 0
+            else:
+                if f(abs(f(calc[i] - m)) / m) <= dos:
+                    pas += 1
+                iz = i // mx
+                ix = i - iz * mx
+                if ix > 0 and pas <= 0 and near(calc[i - 1], m) <= 1:
+                    pas += 1
+                if ix + 1 < mx and pas <= 0 and near(calc[i + 1], m) <= 1:
+                    pas += 1
+                if iz > 0 and near(calc[i - mx], m) <= 1:
+                    pas += 1
+                if iz + 1 < mz and pas <= 0 and near(calc[i + mx], m) <= 1:
+                    pas += 1
+                if pas > 0:
+                    count += 1
+                else:
+                    pas = -1
+        lines.append(f"{m:f}\t {calc[i]:f}\t {pas}")
+    pct = f"{count / total * 100:.0f}" if total else "nan"
+    lines.append(f"Totally {total} points compared, {count} passed, percentage = {pct} %")
+    return lines, total, count
+
+
+def write_relative_dose(base, lines, dims):
+    mx, my, mz = (int(v) for v in dims)
+    name = f"{base}_RelativeDose_{mx:03d}x{my:03d}x{mz:03d}.txt"
+    with open(name, "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    return name
+
+
+def read_measured(path, n):
+    """The measured data file: the first number of each of the first n lines
+    (the reference reads `infile >> v` then skips the rest of the line)."""
+    vals = []
+    for line in Path(path).read_text().splitlines():
+        tok = line.split()
+        if tok:
+            vals.append(float(tok[0]))
+        if len(vals) == n:
+            break
+    if len(vals) < n:
+        raise ValueError(f"measured data {path}: {len(vals)} values, {n} expected")
+    return np.array(vals, np.float32)

@@ -171,6 +171,31 @@ def test_plan_rejects_unsupported_modules(tmp_path):
         load_plan(ini)
 
 
+def test_plan_reads_the_relative_dose_comparison(tmp_path):
+    job = _job()
+    ini = _write_plan(tmp_path, job, extra="""
+[Dose output]
+relative dose = Yes
+starting point = -1.0 0.5 -1.5
+xyz dimensions = 9 1 7
+3d voxel sizes = 0.25 0 0.5
+PTW729/PTW1000 = PTW729
+norm to Max/Center = Center
+gamma index (mm,%) = 3 2
+measured data = "meas.txt"
+""")
+    txt = ini.read_text().replace("isocenter location = 0 0 0", "isocenter location = 0.5 0 -0.25")
+    ini.write_text(txt)
+    rp = load_plan(ini).post["relative"]
+    assert rp["start"] == pytest.approx([-0.5, 0.5, -1.75]) and rp["dims"] == [9, 1, 7]
+    assert rp["array_type"] == 1 and rp["norm_type"] == 2
+    assert rp["gamma_len_cm"] == pytest.approx(0.3) and rp["gamma_dos"] == pytest.approx(0.02)
+    assert rp["measured"].endswith("meas.txt") and "data" in rp["measured"]
+    ini.write_text(txt.replace("gamma index (mm,%) = 3 2\n", ""))
+    with pytest.raises(PlanError, match="gamma index"):
+        load_plan(ini)
+
+
 def test_dose_file_layout(tmp_path):
     d = np.arange(24 * 24 * 12, dtype=np.float32)
     name = F.write_dose(str(tmp_path / "P"), d, 24, 24, 12)
@@ -193,7 +218,16 @@ xyz dimensions = 60 60 20
 absolute dose = Yes
 dose position = 0.1 0.2 0.3
 dose measured = 0
+relative dose = Yes
+starting point = -2.0 0.0 -2.0
+xyz dimensions = 9 1 9
+3d voxel sizes = 0.5 0 0.5
+PTW729/PTW1000 = PTW1000
+norm to Max/Center = Max
+gamma index (mm,%) = 3 3
+measured data = "meas.txt"
 """)
+    (tmp_path / "data" / "meas.txt").write_text("".join(f"{1.0 + 0.01 * i}\n" for i in range(81)))
     name = run_plan(str(ini))
     plan = load_plan(ini)
     ref, _ = oracle.run(plan.job.physics, plan.job.scene(), 0, plan.job.histories)
@@ -201,6 +235,13 @@ dose measured = 0
     np.testing.assert_array_equal(F.read_dose(name).reshape(-1), want)
     log = (tmp_path / "out" / "T1_log.txt").read_text()
     assert "absolute dose at" in log
+    from gegs_b200.postprocess import relative_dose
+    p = plan.job.phantom
+    rel, tot, ok = relative_dose(want, p["x_bounds"], p["y_bounds"], p["z_bounds"], (-2.0, 0.0, -2.0),
+                                 (0.5, 0.0, 0.5), (9, 1, 9), np.float32([1.0 + 0.01 * i for i in range(81)]),
+                                 norm_type=1, array_type=2, gamma_len_cm=0.3, gamma_dos=0.03)
+    assert (tmp_path / "out" / "T1_RelativeDose_009x001x009.txt").read_text().splitlines() == rel
+    assert rel[-1] in log and tot > 0
     from oracle.post_oracle import interp_dose as ref_interp
     grid = np.fromfile(tmp_path / "out" / "T1_Interpolate_060x060x020.bin", np.float32)
     assert grid[:3].view(np.int32).tolist() == [60, 60, 20]

@@ -57,6 +57,83 @@ def test_point_dose_interpolates_between_centres():
     assert point_dose(dose, *b, mid) == pytest.approx(float(dose[3, 4, 5] + dose[3, 4, 6]) / 2, rel=1e-5)
 
 
+def _plane(dose, b, start, sizes, dims):
+    """The voxel whose centre is nearest each point of the comparison plane (ties never occur here)."""
+    c = [(bb[:-1].astype(np.float64) + bb[1:]) / 2 for bb in b]
+    out = []
+    for k in range(dims[2]):
+        for j in range(dims[1]):
+            for i in range(dims[0]):
+                p = [start[a] + sizes[a] * (i, j, k)[a] for a in range(3)]
+                idx = [int(np.argmin(np.abs(c[a] - p[a]))) for a in range(3)]
+                out.append(dose[idx[2], idx[1], idx[0]])
+    return np.array(out, np.float32)
+
+
+def test_relative_dose_samples_and_grades_like_the_detector_array_comparison():
+    from gegs_b200.postprocess import relative_dose, sample_plane
+    rng = np.random.default_rng(5)
+    dose, b = _grid(rng)
+    c = [(bb[:-1] + bb[1:]) / 2 for bb in b]
+    start, sizes, dims = (float(c[0][2]), float(c[1][7]), float(c[2][1])), (0.3, 0.0, 0.5), (12, 1, 6)
+    calc = sample_plane(dose, *b, start, sizes, dims)
+    np.testing.assert_array_equal(calc, _plane(dose, b, start, sizes, dims))
+    lines, tot, ok = relative_dose(dose, *b, start, sizes, dims)
+    assert lines == [f"{v:f}" for v in calc] and tot == ok == 0
+
+    # measured values in cGy (x100 when not normalised): identical except planted misses
+    meas = calc / np.float32(100)
+    meas[[5, 20, 40]] *= np.float32(1.08)
+    meas[30] = np.float32(0.0)                                # below 10 % of the maximum: not compared
+    lines, tot, ok = relative_dose(dose, *b, start, sizes, dims, meas, norm_type=0, array_type=1,
+                                   gamma_len_cm=0.3, gamma_dos=0.03)
+    assert tot == calc.size - 1 and ok == tot - 3
+    flags = [int(l.split()[2]) for l in lines[:-1]]
+    assert flags[5] == flags[20] == flags[40] == -1 and flags[30] == 0
+    assert lines[-1] == f"Totally {tot} points compared, {ok} passed, percentage = {ok / tot * 100:.0f} %"
+
+    # normalised to the maximum: a uniform scale of the measurement changes nothing
+    _, tot1, ok1 = relative_dose(dose, *b, start, sizes, dims, meas * np.float32(3.7), norm_type=1,
+                                 array_type=1, gamma_dos=0.03)
+    assert (tot1, ok1) == (tot, ok)
+
+    # the 1000-chamber array: a miss passes when a neighbour on the row (x) or across rows (z) agrees
+    row = np.full(12 * 6, 2.0, np.float32)
+    calc2 = row.copy()
+    calc2[13] = np.float32(2.2)                                # 10 % off; every neighbour agrees
+    d2 = np.zeros((10, 14, 18), np.float32)
+    lines, tot, ok = relative_dose(_embed(d2, b, start, sizes, dims, calc2), *b, start, sizes, dims,
+                                   row / np.float32(100), array_type=2, gamma_len_cm=0.3, gamma_dos=0.03)
+    assert ok == tot == row.size
+    # with a 2 mm distance criterion the neighbour's 0.25 cm offset alone exceeds it
+    lines, tot, ok = relative_dose(_embed(d2, b, start, sizes, dims, calc2), *b, start, sizes, dims,
+                                   row / np.float32(100), array_type=2, gamma_len_cm=0.2, gamma_dos=0.03)
+    assert ok == tot - 1 and int(lines[13].split()[2]) == -1
+
+
+def _embed(d, b, start, sizes, dims, vals):
+    """A dose grid whose comparison-plane samples are `vals`."""
+    d = d.copy()
+    c = [(bb[:-1].astype(np.float64) + bb[1:]) / 2 for bb in b]
+    n = 0
+    for k in range(dims[2]):
+        for j in range(dims[1]):
+            for i in range(dims[0]):
+                p = [start[a] + sizes[a] * (i, j, k)[a] for a in range(3)]
+                idx = [int(np.argmin(np.abs(c[a] - p[a]))) for a in range(3)]
+                d[idx[2], idx[1], idx[0]] = vals[n]
+                n += 1
+    return d
+
+
+def test_measured_data_file_takes_the_first_number_of_each_line(tmp_path):
+    from gegs_b200.postprocess import read_measured
+    (tmp_path / "m.txt").write_text("1.5 x y\n2.5\n\n3.5 7\n4.5\n")
+    np.testing.assert_array_equal(read_measured(tmp_path / "m.txt", 3), np.float32([1.5, 2.5, 3.5]))
+    with pytest.raises(ValueError):
+        read_measured(tmp_path / "m.txt", 5)
+
+
 @pytest.mark.gpu
 def test_interp_dose_matches_the_oracle():
     from gegs_b200.postprocess import interp_dose
