@@ -127,7 +127,8 @@ def point_dose(dose, x_bounds, y_bounds, z_bounds, pos):
 def sample_plane(dose, x_bounds, y_bounds, z_bounds, start, sizes, dims):
     """The dose of the voxel nearest each point of a comparison grid: the
     reference's index `int((pos - c0) / (c1 - c0) + 0.1)` on voxel centres
-    (output_RelDos_II, output.c:606-624), the + 0.1 in double as in C."""
+    (output_RelDos_II, output.c:606-624), the + 0.1 in double as in C.
+    A point outside the phantom is an error (the reference reads past the grid)."""
     f = np.float32
     d = _f32(dose).reshape(-1)
     nx, ny, nz = len(x_bounds) - 1, len(y_bounds) - 1, len(z_bounds) - 1
@@ -143,6 +144,8 @@ def sample_plane(dose, x_bounds, y_bounds, z_bounds, start, sizes, dims):
                 ix = int(float(f((px - c[0][0]) / f(c[0][1] - c[0][0]))) + 0.1)    # + 0.1 in double
                 iy = int(float(f((py - c[1][0]) / f(c[1][1] - c[1][0]))) + 0.1)
                 iz = int(float(f((pz - c[2][0]) / f(c[2][1] - c[2][0]))) + 0.1)
+                if not (0 <= ix < nx and 0 <= iy < ny and 0 <= iz < nz):
+                    raise ValueError(f"comparison point ({px}, {py}, {pz}) lies outside the phantom")
                 calc[mx * my * k + mx * j + i] = d[nx * ny * iz + nx * iy + ix]
     return calc
 

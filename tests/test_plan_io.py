@@ -219,15 +219,15 @@ absolute dose = Yes
 dose position = 0.1 0.2 0.3
 dose measured = 0
 relative dose = Yes
-starting point = -2.0 0.0 -2.0
-xyz dimensions = 9 1 9
-3d voxel sizes = 0.5 0 0.5
+starting point = -1.0 0.0 -1.2
+xyz dimensions = 9 1 10
+3d voxel sizes = 0.25 0 0.25
 PTW729/PTW1000 = PTW1000
 norm to Max/Center = Max
 gamma index (mm,%) = 3 3
 measured data = "meas.txt"
 """)
-    (tmp_path / "data" / "meas.txt").write_text("".join(f"{1.0 + 0.01 * i}\n" for i in range(81)))
+    (tmp_path / "data" / "meas.txt").write_text("".join(f"{1.0 + 0.01 * i}\n" for i in range(90)))
     name = run_plan(str(ini))
     plan = load_plan(ini)
     ref, _ = oracle.run(plan.job.physics, plan.job.scene(), 0, plan.job.histories)
@@ -237,10 +237,10 @@ measured data = "meas.txt"
     assert "absolute dose at" in log
     from gegs_b200.postprocess import relative_dose
     p = plan.job.phantom
-    rel, tot, ok = relative_dose(want, p["x_bounds"], p["y_bounds"], p["z_bounds"], (-2.0, 0.0, -2.0),
-                                 (0.5, 0.0, 0.5), (9, 1, 9), np.float32([1.0 + 0.01 * i for i in range(81)]),
+    rel, tot, ok = relative_dose(want, p["x_bounds"], p["y_bounds"], p["z_bounds"], (-1.0, 0.0, -1.2),
+                                 (0.25, 0.0, 0.25), (9, 1, 10), np.float32([1.0 + 0.01 * i for i in range(90)]),
                                  norm_type=1, array_type=2, gamma_len_cm=0.3, gamma_dos=0.03)
-    assert (tmp_path / "out" / "T1_RelativeDose_009x001x009.txt").read_text().splitlines() == rel
+    assert (tmp_path / "out" / "T1_RelativeDose_009x001x010.txt").read_text().splitlines() == rel
     assert rel[-1] in log and tot > 0
     from oracle.post_oracle import interp_dose as ref_interp
     grid = np.fromfile(tmp_path / "out" / "T1_Interpolate_060x060x020.bin", np.float32)

@@ -80,6 +80,8 @@ def test_relative_dose_samples_and_grades_like_the_detector_array_comparison():
     np.testing.assert_array_equal(calc, _plane(dose, b, start, sizes, dims))
     lines, tot, ok = relative_dose(dose, *b, start, sizes, dims)
     assert lines == [f"{v:f}" for v in calc] and tot == ok == 0
+    with pytest.raises(ValueError, match="outside"):
+        sample_plane(dose, *b, (float(c[0][-1]) + 1.0, 0.0, 0.0), sizes, (1, 1, 1))
 
     # measured values in cGy (x100 when not normalised): identical except planted misses
     meas = calc / np.float32(100)
