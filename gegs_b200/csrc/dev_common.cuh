@@ -126,6 +126,7 @@ struct DevCtx {
     const float *xb, *yb, *zb;
     const gegs_field *fields;
     const float2 *crossXZ;          // 960
+    const float4 *jaw_lines;        // [field][jaw][8] edge lines of the jaws hownear polygons
     const gegs_phsp_record *phsp;
     unsigned long long *tally;      // int64 MeV*2^30 per voxel
     uint32_t *err;

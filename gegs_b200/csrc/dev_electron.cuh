@@ -332,10 +332,21 @@ __device__ bool electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
         }
         tmxs_val = fminf_(tmxs_val, P->smaxir[medium]);
         tustep = fminf_(tstep, fminf_(tmxs_val, range));
-        bool ok;
-        hownear_g<G>(C, p, tperp, ok);
-        if (!ok) { atomicOr(C.err, GX_ERR_MODULE); return true; }
-        if (P->i_do_rr[medium] == 1 && p.e < P->e_max_rr[medium]) {
+        const bool do_rr = P->i_do_rr[medium] == 1 && p.e < P->e_max_rr[medium];
+        // In the jaws, a lower bound of hownear above the thresholds it is
+        // compared with (range for range rejection, else tustep) decides every
+        // comparison below as the exact value would, and then tustep is left
+        // unchanged: the bound stands in for the value.
+        float lb = -1.0f;
+        if (G == GX_GEOM_JAWS && (p.module == GEGS_M_SECJAWY || p.module == GEGS_M_SECJAWX))
+            lb = jaws_near_lower_bound(C, p);
+        if (lb > (do_rr ? range : tustep)) tperp = lb;
+        else {
+            bool ok;
+            hownear_g<G>(C, p, tperp, ok);
+            if (!ok) { atomicOr(C.err, GX_ERR_MODULE); return true; }
+        }
+        if (do_rr) {
             if (tperp >= range) { e_discard_below_cut(C, p, rd, r); return true; }
         }
         blccl = rhof * P->blcc[medium];

@@ -600,6 +600,34 @@ __device__ void hownear_secjaws_x(const DevCtx &C, const Part &p, float &tperp)
     }
 }
 
+// Lower bound on hownear_secjaws_y / _x: their result is a minimum over
+// distances to some of three (point, polygon) pairs -- the bounding polygon
+// seen from (y, z) and from (x, z), and the jaw opening seen from (x, z) for
+// the Y jaws or from (y, z) for the X jaws -- and a distance to a polygon is
+// at least the distance to the line of its nearest edge. 10 um covers the
+// rounding of both sides at coordinates up to 100 cm (a few 1e-5 cm). Every
+// lane evaluates the same twelve lines, so a warp whose steps are all shorter
+// than the bound skips the exact polygon distances as a whole.
+__device__ __forceinline__ float jaws_near_lower_bound(const DevCtx &C, const Part &p)
+{
+    const bool xjaw = p.module == GEGS_M_SECJAWX;
+    const float4 *L = C.jaw_lines + ((size_t)p.field * 2 + (xjaw ? 1 : 0)) * 8;
+    float m = __int_as_float(0x7f7fffff);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float4 l = __ldg(&L[k]);
+        m = fminf(m, fabsf(l.x * p.y + l.y * p.z - l.z));
+        m = fminf(m, fabsf(l.x * p.x + l.y * p.z - l.z));
+    }
+    const float qx = xjaw ? p.y : p.x;
+#pragma unroll
+    for (int k = 4; k < 8; k++) {
+        const float4 l = __ldg(&L[k]);
+        m = fminf(m, fabsf(l.x * qx + l.y * p.z - l.z));
+    }
+    return m - 1e-3f;
+}
+
 // dispatch on the particle's module (photon.cu:142-158, electron.cu:1491-1508)
 __device__ __forceinline__ uint32_t howfar(const DevCtx &C, Part &p, float &t, bool &ok)
 {

@@ -1,6 +1,7 @@
 // Host engine behind the C ABI (include/gegs.h): device buffers, the event
 // queues, the persistent CUDA-graph wave loop and the plain host-driven loop.
 #include <cuda_runtime.h>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -48,6 +49,7 @@ struct gegs_engine {
     float *d_xb = nullptr, *d_yb = nullptr, *d_zb = nullptr;
     gegs_field *d_fields = nullptr;
     float2 *d_cross = nullptr;
+    float4 *d_jaw_lines = nullptr;      // per field and jaw: 8 unit edge lines (jaws hownear bound)
     gegs_phsp_record *d_phsp = nullptr;
     uint64_t nphsp = 0, phsp_cap = 0;
     unsigned long long *d_tally = nullptr;
@@ -108,6 +110,36 @@ static cudaError_t realloc_dev(T **p, size_t n)
     return cudaMalloc((void **)p, n * sizeof(T));
 }
 
+// Unit normal form (a, b, c), a*x + b*y = c, of the line through each edge of
+// the polygons that hownear_secjaws_y / _x measure (the bounding polygon and
+// the jaw opening), per field and jaw: [field][jaw: Y, X][8]. |a*x + b*y - c|
+// is at most the distance to the edge, so the smallest over the eight lines
+// bounds hownear from below (jaws_near_lower_bound). A zero-length edge gets
+// a line through its point.
+static std::vector<float4> jaw_edge_lines(const gegs_field *F, int nfields)
+{
+    std::vector<float4> out((size_t)(nfields > 0 ? nfields : 0) * 16);
+    auto line = [](const float (*poly)[2], int i) {
+        const double ax = poly[i][0], ay = poly[i][1];
+        const double bx = poly[(i + 1) & 3][0], by = poly[(i + 1) & 3][1];
+        double nx = -(by - ay), ny = bx - ax;
+        double len = std::sqrt(nx * nx + ny * ny);
+        if (len == 0.0) { nx = 1.0; ny = 0.0; len = 1.0; }
+        nx /= len; ny /= len;
+        return make_float4((float)nx, (float)ny, (float)(nx * ax + ny * ay), 0.0f);
+    };
+    for (int f = 0; f < nfields; f++) {
+        float4 *o = out.data() + (size_t)f * 16;
+        for (int i = 0; i < 4; i++) {
+            o[i] = line(F[f].boundMaxY, i);
+            o[4 + i] = line(F[f].jawsGeomY + 2, i);
+            o[8 + i] = line(F[f].boundMaxX, i);
+            o[12 + i] = line(F[f].jawsGeomX + 2, i);
+        }
+    }
+    return out;
+}
+
 extern "C" {
 
 const char *gegs_version(void) { return "gegs_b200 0.1 (sm_100a)"; }
@@ -151,7 +183,7 @@ void gegs_destroy(gegs_engine *e)
     for (int k = 0; k < 2; k++) if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
     cudaFree(e->d_blw); cudaFree(e->d_gvm); cudaFree(e->d_grad);
     cudaFree(e->d_P); cudaFree(e->d_reg); cudaFree(e->d_xb); cudaFree(e->d_yb); cudaFree(e->d_zb);
-    cudaFree(e->d_fields); cudaFree(e->d_cross); cudaFree(e->d_phsp); cudaFree(e->d_tally);
+    cudaFree(e->d_fields); cudaFree(e->d_cross); cudaFree(e->d_jaw_lines); cudaFree(e->d_phsp); cudaFree(e->d_tally);
     cudaFree(e->d_err); cudaFree(e->d_stats); cudaFree(e->d_sched); cudaFree(e->d_qmeta);
     cudaFree(e->d_trace); cudaFree(e->d_trace_n);
     for (int q = 0; q < GX_NQ; q++) cudaFree(e->d_qbuf[q]);
@@ -233,6 +265,12 @@ gegs_status gegs_set_scene(gegs_engine *e, const gegs_scene *S)
     CK(cudaMemcpy(e->d_zb, S->z_bounds, ((size_t)S->nz + 1) * 4, cudaMemcpyHostToDevice), "bounds H2D");
     CK(realloc_dev(&e->d_fields, (size_t)S->nfields), "fields");
     CK(cudaMemcpy(e->d_fields, S->fields, sizeof(gegs_field) * S->nfields, cudaMemcpyHostToDevice), "fields H2D");
+    {
+        std::vector<float4> lines = jaw_edge_lines(S->fields, S->nfields);
+        CK(realloc_dev(&e->d_jaw_lines, lines.size()), "jaw lines");
+        CK(cudaMemcpy(e->d_jaw_lines, lines.data(), lines.size() * sizeof(float4), cudaMemcpyHostToDevice),
+           "jaw lines H2D");
+    }
     if (!e->d_cross) CK(cudaMalloc(&e->d_cross, sizeof(float2) * 960), "crossXZ");
     CK(cudaMemcpy(e->d_cross, S->crossXZ, sizeof(float2) * 960, cudaMemcpyHostToDevice), "crossXZ H2D");
     if (nvox != e->nvox || !e->d_tally) {
@@ -250,6 +288,7 @@ gegs_status gegs_set_scene(gegs_engine *e, const gegs_scene *S)
     C.xb = e->d_xb; C.yb = e->d_yb; C.zb = e->d_zb;
     C.fields = e->d_fields;
     C.crossXZ = e->d_cross;
+    C.jaw_lines = e->d_jaw_lines;
     C.phsp = e->d_phsp;
     C.nphsp = e->nphsp;
     C.tally = e->d_tally;
