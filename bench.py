@@ -117,19 +117,28 @@ def algorithmic_bytes(job, sample):
 
 
 def cpu_histories_per_s(job, seconds=15.0, threads=None):
-    """Oracle throughput on the host cores over a bounded sample (~`seconds`)."""
+    """Oracle throughput on the host cores over a bounded sample (~`seconds`):
+    a warm-up run (thread pool, first touches), then samples growing 4x until
+    one takes a second, then one run sized to `seconds`."""
     from oracle import oracle as O
     threads = threads or os.cpu_count()
     sh = job.scene()
     n = 2000
-    t = time.perf_counter()
     O.run(job.physics, sh, 0, n, threads=threads)
-    dt = time.perf_counter() - t
-    n2 = int(max(n, min(2_000_000, n * seconds / max(dt, 1e-3))))
-    t = time.perf_counter()
-    O.run(job.physics, sh, 0, n2, threads=threads)
-    dt = time.perf_counter() - t
-    return n2 / dt, n2, dt, threads
+    while True:
+        t = time.perf_counter()
+        O.run(job.physics, sh, 0, n, threads=threads)
+        dt = time.perf_counter() - t
+        if dt >= min(1.0, seconds / 4) or n >= 1_000_000:
+            break
+        n *= 4
+    n2 = int(min(4_000_000, n * seconds / max(dt, 1e-3)))
+    if n2 > n:
+        t = time.perf_counter()
+        O.run(job.physics, sh, 0, n2, threads=threads)
+        dt = time.perf_counter() - t
+        n = n2
+    return n / dt, n, dt, threads
 
 
 def c4_gradient(args, eng):
@@ -197,11 +206,44 @@ def c5_batch(args, device):
     pb.run_sequential()
     seq = pb.wall_s
     pb.close()
-    return {"workload": f"C5: {len(jobs)} plans (slab and CT head, 16^3..256x256x128 voxels, 1-7 fields), "
-                        f"histories log-uniform {args.c5_hist_max // 100}..{args.c5_hist_max}",
-            "histories": total, "concurrent_s": conc, "sequential_s": seq,
-            "concurrent_histories_per_s": total / conc, "sequential_histories_per_s": total / seq,
-            "timing": "host wall clock from the first launch to the last wait"}
+    out = {"workload": f"C5: {len(jobs)} plans (slab and CT head, 16^3..256x256x128 voxels, 1-7 fields), "
+                       f"histories log-uniform {args.c5_hist_max // 100}..{args.c5_hist_max}",
+           "histories": total, "concurrent_s": conc, "sequential_s": seq,
+           "concurrent_histories_per_s": total / conc, "sequential_histories_per_s": total / seq,
+           "timing": "host wall clock from the first launch to the last wait"}
+    if args.c5_descent_iterations > 0:
+        out["descent"] = c5_descent(args, device)
+    return out
+
+
+def c5_descent(args, device):
+    """Gradient descent on the beamlet weights of 4 plans at once (CT heads of
+    four sizes, 5 fields x 20 x 20 beamlets): every iteration runs the four
+    forward transports concurrently, then each plan's replay backward."""
+    from gegs_b200 import workloads as W
+    from gegs_b200.differentiable import BeamletModel, optimize_weights_batch
+    from gegs_b200.engine import Engine
+    dims = [(64, 64, 48), (96, 96, 64), (128, 128, 96), (256, 256, 120)]
+    h = args.c5_descent_histories
+    models, engines, w0s, targets, organs = [], [], [], [], []
+    for k, d in enumerate(dims):
+        job = W.config4(histories=h, nphsp=1_000_000, dims=d, seed=W.SEED_BASE + 40 + k)
+        e = Engine(device)
+        e.set_physics(job.physics)
+        e.set_scene(job.scene())
+        m = BeamletModel(e, job, batch=1 << 20)
+        w0 = job.beam["beamlets"]["weights"].astype(np.float64)
+        m.calibrate(w0, job.meta["target"], 50.0)
+        models.append(m); engines.append(e); w0s.append(w0)
+        targets.append(job.meta["target"]); organs.append(job.meta["organ"])
+    t0 = time.perf_counter()
+    _, hist = optimize_weights_batch(models, w0s, targets, organs, iterations=args.c5_descent_iterations)
+    wall = time.perf_counter() - t0
+    for e in engines:
+        e.close()
+    return {"plans": [f"CT head {d[0]}x{d[1]}x{d[2]}, 5 fields x 20x20 beamlets" for d in dims],
+            "iterations": args.c5_descent_iterations, "histories_per_iteration": h, "wall_s": wall,
+            "objective_first": [x[0] for x in hist], "objective_last": [x[-1] for x in hist]}
 
 
 def make_job(args, histories):
@@ -266,6 +308,9 @@ def main():
     ap.add_argument("--c4-iterations", type=int, default=20)
     ap.add_argument("--c5-plans", type=int, default=32, help="plans of the batched sweep (0: skip)")
     ap.add_argument("--c5-hist-max", type=int, default=10_000_000)
+    ap.add_argument("--c5-descent-iterations", type=int, default=20,
+                    help="gradient-descent iterations on 4 plans at once (0: skip)")
+    ap.add_argument("--c5-descent-histories", type=int, default=1_000_000)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -427,8 +472,10 @@ def main():
     cpu = None
     if not args.no_cpu:
         crate, cn, cdt, cores = cpu_histories_per_s(job, seconds=args.cpu_seconds)
+        r1, n1, dt1, _ = cpu_histories_per_s(job, seconds=3.0, threads=1)
         cpu = {"value": crate, "unit": "histories/s", "cores": cores, "kind": "port",
-               "sample": f"{cn} C3 histories in {cdt:.1f} s on {cores} host threads (CPU oracle, same inputs)"}
+               "sample": f"{cn} C3 histories in {cdt:.1f} s on {cores} host threads (CPU oracle, same inputs)",
+               "value_1_core": r1, "sample_1_core": f"{n1} C3 histories in {dt1:.1f} s on 1 thread"}
     # per step: the first planner launch, then per wave the source, the stage kernels (the
     # persistent form runs photon and electron transport as jaws + MLC + phantom kernels) and the planner
     per_wave = 12 if args.mode == "plain" else 16

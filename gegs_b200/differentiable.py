@@ -45,6 +45,19 @@ class BeamletModel:
         self.forward_ms = st["device_ms"]
         return e.tally().astype(np.float64) * (FIXED * self.unit) / self.mass
 
+    def launch_dose(self, w):
+        """Queue the forward transport at weights w and return at once; dose
+        plans on other engines can be queued before finish_dose."""
+        e = self.engine
+        e.set_beamlet_weights(np.asarray(w, np.float32))
+        e.reset_tally()
+        e.launch(self.h0, self.h1, batch=self.batch)
+
+    def finish_dose(self) -> np.ndarray:
+        st = self.engine.wait()
+        self.forward_ms = st["device_ms"]
+        return self.engine.tally().astype(np.float64) * (FIXED * self.unit) / self.mass
+
     def vjp(self, dL_dD) -> np.ndarray:
         """dL/dw from dL/dD (per voxel)."""
         g = np.asarray(dL_dD, np.float64).reshape(-1) * (self.unit / self.mass)
@@ -132,3 +145,26 @@ def optimize_weights(model: BeamletModel, w0, target, organ, iterations=20, lr=0
             w -= step * g
             w.clamp_(min=0.0)
     return w.detach().numpy(), history
+
+
+def optimize_weights_batch(models, w0s, targets, organs, iterations=20, lr=0.05, prescription=60.0, limit=20.0):
+    """optimize_weights on several plans at once: every iteration queues the
+    forward transport of all plans (each engine on its own stream, so they run
+    concurrently on the device), then takes each plan's objective, its replay
+    backward and its projected step. Returns the final weights and the
+    objective history of every plan."""
+    ws = [np.asarray(w, np.float64).copy() for w in w0s]
+    hist = [[] for _ in models]
+    for _ in range(iterations):
+        for m, w in zip(models, ws):
+            m.launch_dose(w)
+        doses = [m.finish_dose() for m in models]
+        for k, (m, d) in enumerate(zip(models, doses)):
+            dt = torch.from_numpy(d).requires_grad_(True)
+            loss = objective(dt, targets[k], organs[k], prescription, limit)
+            loss.backward()
+            hist[k].append(float(loss))
+            g = m.vjp(dt.grad.numpy())
+            step = lr * float(np.abs(ws[k]).mean()) / max(float(np.abs(g).max()), 1e-30)
+            ws[k] = np.maximum(ws[k] - step * g, 0.0)
+    return ws, hist

@@ -89,3 +89,33 @@ def test_gradient_descent_lowers_the_objective(engine):
     w, hist = optimize_weights(model, w0, job.meta["target"], job.meta["organ"], iterations=8)
     assert len(hist) == 8 and hist[-1] < hist[0]
     assert (w >= 0).all()
+
+
+@pytest.mark.gpu
+def test_descent_on_several_plans_at_once_matches_one_plan_at_a_time(engine):
+    from gegs_b200.differentiable import BeamletModel, optimize_weights, optimize_weights_batch
+    from gegs_b200.engine import Engine
+    jobs = [_job(4000), W.config4(histories=4000, nphsp=6000, dims=(40, 40, 20), nb=8, bixel=1.25,
+                                  seed=W.SEED_BASE + 77)]
+    jobs[1].meta["organ"] = W.ellipsoid_mask(jobs[1], (1.0, 0.5, 0.0), (0.8, 0.8, 1.0))
+    engines, models, w0s = [], [], []
+    try:
+        for job in jobs:
+            e = Engine(0)
+            e.set_physics(job.physics)
+            e.set_scene(job.scene())
+            m = BeamletModel(e, job, batch=1 << 16)
+            w0 = job.beam["beamlets"]["weights"].astype(np.float64)
+            m.calibrate(w0, job.meta["target"], 50.0)
+            engines.append(e); models.append(m); w0s.append(w0)
+        targets = [j.meta["target"] for j in jobs]
+        organs = [j.meta["organ"] for j in jobs]
+        ws, hist = optimize_weights_batch(models, w0s, targets, organs, iterations=4)
+        for k in range(len(jobs)):
+            w1, h1 = optimize_weights(models[k], w0s[k], targets[k], organs[k], iterations=4)
+            np.testing.assert_allclose(hist[k], h1, rtol=1e-9)
+            np.testing.assert_allclose(ws[k], w1, rtol=1e-9, atol=1e-12)
+            assert hist[k][-1] < hist[k][0]
+    finally:
+        for e in engines:
+            e.close()
