@@ -467,6 +467,8 @@ def main():
 
     # ---- C4: beamlet gradient by replay vs forward and finite differences ---
     grad = c4_gradient(args, eng) if args.c4_histories > 0 else None
+    nvox = eng.nvox
+    eng.close()                                    # its event queues (up to ~74 GB) before the C5 engines
     batched = c5_batch(args, local) if args.c5_plans > 0 else None
 
     cpu = None
@@ -490,7 +492,7 @@ def main():
                    "hist_per_step": H, "mode": args.mode, "parallelism": f"histories sharded over {world} GPU(s)",
                    "l2": "working set (63 MB region table + 63 MB int64 tally + event queues) exceeds the 126 MB L2; no flush"},
         "e2e": {"value": e2e, "unit": "histories/s", "h2d_bytes_per_step": rec_per_step * 28,
-                "d2h_bytes_per_step": eng.nvox * 8},
+                "d2h_bytes_per_step": nvox * 8},
         "roofline": {"bound": "hbm", "kernel": f"{dom_name} transport (k_{dom_name}_jaws + k_{dom_name}_mlc + k_{dom_name}, one wave)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": tr,
