@@ -21,7 +21,44 @@ from pathlib import Path
 import numpy as np
 
 
-def run_plan(ini, device=0, max_histories=None, out=sys.stdout):
+def transport_in_batches(eng, fields, output_factors, nbatch):
+    """Every field's histories split into `nbatch` equal parts; batch b runs
+    part b of every field. Returns the energy (the same float64 expression of
+    the same int64 tallies as an unbatched run) and the relative standard error
+    of its mean per voxel from the batch energies, with the reference's batch
+    formula sqrt((S2/n - (S1/n)^2) / (n - 1)) / (S1/n) (CUDA_EGS.cu:817-876;
+    its last, partial batch has no counterpart here: the batches are equal)."""
+    acc = [np.zeros(eng.nvox, np.int64) for _ in fields]
+    s1 = np.zeros(eng.nvox, np.float64)
+    s2 = np.zeros(eng.nvox, np.float64)
+    for b in range(nbatch):
+        eb = np.zeros(eng.nvox, np.float64)
+        for k, (f, of) in enumerate(zip(fields, output_factors)):
+            h0, h1 = int(f["hist_begin"]), int(f["hist_end"])
+            lo = h0 + (h1 - h0) * b // nbatch
+            hi = h0 + (h1 - h0) * (b + 1) // nbatch
+            if hi <= lo:
+                continue
+            eng.reset_tally()
+            eng.run(lo, hi)
+            t = eng.tally()
+            acc[k] += t
+            eb += t.astype(np.float64) * of
+        s1 += eb
+        s2 += eb * eb
+    n = float(nbatch)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        sigma = np.sqrt(np.maximum(s2 / n - (s1 / n) ** 2, 0.0) / (n - 1.0)) / (s1 / n)
+    if all(abs(of - 1.0) < 1e-12 for of in output_factors):
+        energy = np.sum(acc, axis=0).astype(np.float64)
+    else:
+        energy = np.zeros(eng.nvox, np.float64)
+        for a, of in zip(acc, output_factors):
+            energy += a.astype(np.float64) * of
+    return energy, sigma
+
+
+def run_plan(ini, device=0, max_histories=None, out=sys.stdout, uncertainty_batches=0):
     from . import build as B
     from . import io_formats as F
     from .plan import load_plan
@@ -33,7 +70,12 @@ def run_plan(ini, device=0, max_histories=None, out=sys.stdout):
     eng.set_physics(job.physics)
     eng.set_scene(job.scene())
     t0 = time.perf_counter()
-    if all(abs(f - 1.0) < 1e-12 for f in plan.field_output_factors):
+    sigma = None
+    if uncertainty_batches:
+        if uncertainty_batches < 2:
+            raise ValueError("the batch uncertainty needs at least 2 batches")
+        energy, sigma = transport_in_batches(eng, job.fields, plan.field_output_factors, uncertainty_batches)
+    elif all(abs(f - 1.0) < 1e-12 for f in plan.field_output_factors):
         eng.run(0, job.histories)
         energy = eng.tally().astype(np.float64)
     else:
@@ -48,6 +90,9 @@ def run_plan(ini, device=0, max_histories=None, out=sys.stdout):
     name = F.write_dose(plan.output_base, dose.astype(np.float32), plan.nx, plan.ny, plan.nz)
     st = eng.stats()
     extra = []
+    if sigma is not None:
+        un = F.write_uncertainty(plan.output_base, sigma.astype(np.float32), plan.nx, plan.ny, plan.nz)
+        extra.append(f"uncertainty ({uncertainty_batches} batches) {un}")
     p = job.phantom
     bounds = (p["x_bounds"], p["y_bounds"], p["z_bounds"])
     if "interp" in plan.post:
@@ -94,8 +139,11 @@ def main(argv=None):
     ap.add_argument("-i", "--input", required=True, help="plan in the reference's INI format")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--max-histories", type=int, default=None, help="cap the histories of each field")
+    ap.add_argument("--uncertainty", type=int, default=0, metavar="BATCHES",
+                    help="also write the relative standard error per voxel from this many batches "
+                         "(the reference's GET_UNCERTAINTY output)")
     a = ap.parse_args(argv)
-    run_plan(a.input, a.device, a.max_histories)
+    run_plan(a.input, a.device, a.max_histories, uncertainty_batches=a.uncertainty)
 
 
 if __name__ == "__main__":

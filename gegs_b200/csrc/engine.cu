@@ -674,6 +674,15 @@ extern "C" gegs_status gegs_get_tally(gegs_engine *e, int64_t *out, uint64_t nvo
     return GEGS_OK;
 }
 
+extern "C" gegs_status gegs_set_tally(gegs_engine *e, const int64_t *in, uint64_t nvox)
+{
+    if (!e || !in || nvox != e->nvox || !e->d_tally) return GEGS_ERR_ARG;
+    if (e->in_flight) { e->err = "a launched run has not been waited for (gegs_wait)"; return GEGS_ERR_ARG; }
+    CK(cudaMemcpyAsync(e->d_tally, in, nvox * 8, cudaMemcpyHostToDevice, e->stream), "tally H2D");
+    CK(cudaStreamSynchronize(e->stream), "tally sync");
+    return GEGS_OK;
+}
+
 extern "C" gegs_status gegs_get_dose(gegs_engine *e, const float *voxel_mass, double dose_unit, double *out, uint64_t nvox)
 {
     if (!e || !out || !voxel_mass || nvox != e->nvox || !e->d_tally) return GEGS_ERR_ARG;

@@ -19,7 +19,7 @@ STATUS = {0: "GEGS_OK", 1: "GEGS_ERR_ARG", 2: "GEGS_ERR_CUDA", 3: "GEGS_ERR_QUEU
 MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 
 EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
-           "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_get_dose", "gegs_get_stats",
+           "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_set_tally", "gegs_get_dose", "gegs_get_stats",
            "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version"]
 
 
@@ -72,6 +72,7 @@ def load_library(path=None):
     L.gegs_backward.argtypes = [vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint32, C.POINTER(RunOpts)]
     L.gegs_reset_tally.argtypes = [vp]
     L.gegs_get_tally.argtypes = [vp, vp, C.c_uint64]
+    L.gegs_set_tally.argtypes = [vp, vp, C.c_uint64]
     L.gegs_get_dose.argtypes = [vp, vp, C.c_double, vp, C.c_uint64]
     L.gegs_get_stats.argtypes = [vp, C.POINTER(RunStats)]
     L.gegs_tally_device_ptr.argtypes = [vp, C.POINTER(vp)]
@@ -171,6 +172,25 @@ class Engine:
         out = np.zeros(self.nvox, np.int64)
         self._check(self.L.gegs_get_tally(self.h, out.ctypes.data, self.nvox))
         return out
+
+    def set_tally(self, tally: np.ndarray):
+        t = np.ascontiguousarray(tally, np.int64)
+        if t.size != self.nvox:
+            raise ValueError(f"tally of {t.size} voxels, the scene has {self.nvox}")
+        self._check(self.L.gegs_set_tally(self.h, t.ctypes.data, self.nvox))
+
+    def checkpoint(self, path, next_history: int):
+        """Save the tally and the index of the next history to run (.npz)."""
+        np.savez(path, tally=self.tally(), next_history=np.uint64(next_history), nvox=np.uint64(self.nvox))
+
+    def resume(self, path) -> int:
+        """Load a checkpoint's tally; returns the next history to run. Running
+        the remaining histories then gives the whole run's tally bit for bit."""
+        with np.load(path) as z:
+            if int(z["nvox"]) != self.nvox:
+                raise ValueError("checkpoint of another phantom")
+            self.set_tally(z["tally"])
+            return int(z["next_history"])
 
     def dose(self, voxel_mass: np.ndarray, dose_unit: float = 1.6e-8) -> np.ndarray:
         m = np.ascontiguousarray(voxel_mass, np.float32)

@@ -434,6 +434,18 @@ def write_dose(base, dose, nx, ny, nz):
     return name
 
 
+def write_uncertainty(base, sigma, nx, ny, nz):
+    """Raw float32 relative uncertainty per voxel, x fastest, under the
+    reference's file name `<base>_uncertianty_NNNxNNNxNNN.bin` (its spelling,
+    output.c:920-944); returns the file name."""
+    d = np.ascontiguousarray(sigma, np.float32).reshape(-1)
+    if d.size != nx * ny * nz:
+        raise ValueError("uncertainty size does not match the phantom")
+    name = f"{base}_uncertianty_{nx:03d}x{ny:03d}x{nz:03d}.bin"
+    d.tofile(name)
+    return name
+
+
 def read_dose(path):
     m = re.search(r"_DoseResults_(\d+)x(\d+)x(\d+)\.bin$", str(path))
     if not m:

@@ -158,6 +158,12 @@ gegs_status gegs_reset_tally(gegs_engine *e);
 /* Copy the int64 tally (nvox entries) to host memory. */
 gegs_status gegs_get_tally(gegs_engine *e, int64_t *out, uint64_t nvox);
 
+/* Load the int64 tally from host memory (no counterpart in the reference,
+ * which has no checkpoint). A checkpoint is the tally and the next history
+ * index: loading it and running the remaining histories gives the tally of
+ * the whole run bit for bit (per-history random streams, integer sums). */
+gegs_status gegs_set_tally(gegs_engine *e, const int64_t *in, uint64_t nvox);
+
 /* dose[i] = tally[i] * 2^-30 / voxel_mass[i] * dose_unit, in double, on the device;
  * voxel_mass is a host array of nvox entries (0 treated as 1, init.cu:1256-1271). */
 gegs_status gegs_get_dose(gegs_engine *e, const float *voxel_mass, double dose_unit, double *out, uint64_t nvox);

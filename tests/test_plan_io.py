@@ -228,7 +228,7 @@ gamma index (mm,%) = 3 3
 measured data = "meas.txt"
 """)
     (tmp_path / "data" / "meas.txt").write_text("".join(f"{1.0 + 0.01 * i}\n" for i in range(90)))
-    name = run_plan(str(ini))
+    name = run_plan(str(ini), uncertainty_batches=4)
     plan = load_plan(ini)
     ref, _ = oracle.run(plan.job.physics, plan.job.scene(), 0, plan.job.histories)
     want = (ref.astype(np.float64) * 2.0 ** -30 / plan.job.voxel_mass() * plan.dose_unit).astype(np.float32)
@@ -242,6 +242,9 @@ measured data = "meas.txt"
                                  norm_type=1, array_type=2, gamma_len_cm=0.3, gamma_dos=0.03)
     assert (tmp_path / "out" / "T1_RelativeDose_009x001x010.txt").read_text().splitlines() == rel
     assert rel[-1] in log and tot > 0
+    sig = np.fromfile(tmp_path / "out" / "T1_uncertianty_024x024x012.bin", np.float32)
+    dosed = want > 0.5 * want.max()
+    assert np.isfinite(sig[dosed]).all() and 0 < np.median(sig[dosed]) < 1
     from oracle.post_oracle import interp_dose as ref_interp
     grid = np.fromfile(tmp_path / "out" / "T1_Interpolate_060x060x020.bin", np.float32)
     assert grid[:3].view(np.int32).tolist() == [60, 60, 20]
@@ -249,3 +252,44 @@ measured data = "meas.txt"
     np.testing.assert_array_equal(grid[3:].reshape(20, 60, 60),
                                   ref_interp(want, p["x_bounds"], p["y_bounds"], p["z_bounds"],
                                              (-2.3, -2.3, -2.9), (0.08, 0.08, 0.3), (60, 60, 20)))
+
+
+class _FakeEngine:
+    """Tally of a history range: voxel v gets sum over h of ((3 h + v) mod 5) * 2^20."""
+    nvox = 6
+
+    def __init__(self):
+        self.t = np.zeros(self.nvox, np.int64)
+
+    def reset_tally(self):
+        self.t[:] = 0
+
+    def run(self, lo, hi):
+        h = np.arange(lo, hi, dtype=np.int64)[:, None]
+        self.t += (((3 * h + np.arange(self.nvox)) % 5) << 20).sum(axis=0)
+
+    def tally(self):
+        return self.t.copy()
+
+
+def test_batch_uncertainty_splits_every_field_and_keeps_the_tally(tmp_path):
+    from gegs_b200.__main__ import transport_in_batches
+    fields = [dict(hist_begin=0, hist_end=100), dict(hist_begin=100, hist_end=250)]
+    of = [1.0, 0.5]
+    energy, sigma = transport_in_batches(_FakeEngine(), fields, of, 5)
+    e = _FakeEngine()
+    whole = np.zeros(6)
+    batches = np.zeros((5, 6))
+    for k, f in enumerate(fields):
+        e.reset_tally(); e.run(f["hist_begin"], f["hist_end"]); whole += e.tally() * of[k]
+        n = f["hist_end"] - f["hist_begin"]
+        for b in range(5):
+            e.reset_tally(); e.run(f["hist_begin"] + n * b // 5, f["hist_begin"] + n * (b + 1) // 5)
+            batches[b] += e.tally() * of[k]
+    np.testing.assert_array_equal(energy, whole)
+    m = batches.mean(axis=0)
+    want = np.sqrt(np.maximum((batches ** 2).mean(axis=0) - m * m, 0) / 4) / m
+    np.testing.assert_allclose(sigma, want, rtol=1e-12)
+    name = F.write_uncertainty(str(tmp_path / "U"), sigma.astype(np.float32), 1, 2, 3)
+    assert name.endswith("U_uncertianty_001x002x003.bin")
+    np.testing.assert_array_equal(np.fromfile(name, np.float32), sigma.astype(np.float32))
