@@ -57,6 +57,9 @@ struct gegs_engine {
     uint32_t *d_err = nullptr;
     unsigned long long *d_stats = nullptr;
     SchedState *d_sched = nullptr;
+    unsigned long long *d_timeline = nullptr;   // wave timeline (gegs_set_timeline)
+    uint32_t timeline_waves = 0;
+    std::vector<unsigned long long> timeline_init;
     TraceRec *d_trace = nullptr;
     uint32_t *d_trace_n = nullptr;
     uint32_t trace_cap = 0;
@@ -183,6 +186,7 @@ void gegs_destroy(gegs_engine *e)
     for (int k = 0; k < 2; k++) if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
     cudaFree(e->d_blw); cudaFree(e->d_gvm); cudaFree(e->d_grad);
     cudaFree(e->d_P); cudaFree(e->d_reg); cudaFree(e->d_xb); cudaFree(e->d_yb); cudaFree(e->d_zb);
+    cudaFree(e->d_timeline);
     cudaFree(e->d_fields); cudaFree(e->d_cross); cudaFree(e->d_jaw_lines); cudaFree(e->d_phsp); cudaFree(e->d_tally);
     cudaFree(e->d_err); cudaFree(e->d_stats); cudaFree(e->d_sched); cudaFree(e->d_qmeta);
     cudaFree(e->d_trace); cudaFree(e->d_trace_n);
@@ -506,6 +510,16 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
     CK(cudaMemsetAsync(e->d_qmeta, 0, sizeof(uint32_t) * 3 * GX_NQ, e->stream), "qmeta reset");
     CK(cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->stream), "err reset");
     CK(cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 16, e->stream), "stats reset");
+    if (e->d_timeline) {
+        // start stamps at the maximum, end stamps at 0 (each wave x kernel pair)
+        e->timeline_init.resize((size_t)e->timeline_waves * 32);
+        for (size_t i = 0; i < e->timeline_init.size(); i += 2) {
+            e->timeline_init[i] = ~0ull;
+            e->timeline_init[i + 1] = 0ull;
+        }
+        CK(cudaMemcpyAsync(e->d_timeline, e->timeline_init.data(), e->timeline_init.size() * 8,
+                           cudaMemcpyHostToDevice, e->stream), "timeline reset");
+    }
 
     for (int k = 0; k < 16; k++) { e->last.stage_ms[k] = 0.0; e->last.stage_launches[k] = 0; }
     if (o.mode == GEGS_MODE_PERSISTENT) {
@@ -700,6 +714,33 @@ extern "C" gegs_status gegs_get_dose(gegs_engine *e, const float *voxel_mass, do
     return GEGS_OK;
 }
 
+extern "C" gegs_status gegs_set_timeline(gegs_engine *e, uint32_t max_waves)
+{
+    if (!e) return GEGS_ERR_ARG;
+    if (e->in_flight) { e->err = "a launched run has not been waited for (gegs_wait)"; return GEGS_ERR_ARG; }
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    cudaFree(e->d_timeline);
+    e->d_timeline = nullptr;
+    e->timeline_waves = 0;
+    if (max_waves) {
+        CK(cudaMalloc(&e->d_timeline, (size_t)max_waves * 32 * sizeof(unsigned long long)), "timeline");
+        e->timeline_waves = max_waves;
+    }
+    e->ctx.timeline = e->d_timeline;
+    e->ctx.timeline_waves = e->timeline_waves;
+    e->ctx_gen++;
+    return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_get_timeline(gegs_engine *e, uint64_t *out, uint32_t max_waves)
+{
+    if (!e || !out || !e->d_timeline) return GEGS_ERR_ARG;
+    uint32_t m = max_waves < e->timeline_waves ? max_waves : e->timeline_waves;
+    CK(cudaMemcpy(out, e->d_timeline, (size_t)m * 32 * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+       "timeline D2H");
+    return GEGS_OK;
+}
+
 extern "C" gegs_status gegs_set_trace(gegs_engine *e, uint32_t capacity)
 {
     if (!e) return GEGS_ERR_ARG;
@@ -827,6 +868,8 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
     c.err = err;
     c.stats = stats;
     c.wave = &sched->waves;
+    c.timeline = nullptr;
+    c.timeline_waves = 0;
     c.trace = nullptr;
     c.trace_n = nullptr;
     c.trace_cap = 0;

@@ -25,6 +25,26 @@ struct SchedState {
     uint32_t refill_below;
 };
 
+// ---- wave timeline (tracing; off unless DevCtx::timeline is set) ------------
+// Kernel ids: 0 source; 1-3 photon jaws / MLC / phantom; 4-7 Compton, photo,
+// Rayleigh, pair; 8-10 electron jaws / MLC / phantom; 11-14 Moller, brems,
+// Bhabha, annihilation. Each block's thread 0 lowers the kernel's start stamp
+// of this wave when the block begins and raises its end stamp once the block
+// is done (after the block's barrier).
+enum : int { TL_SOURCE = 0, TL_PHOTON = 1, TL_PINT = 4, TL_ELECTRON = 8, TL_EINT = 11 };
+
+__device__ __forceinline__ void timeline_mark(const DevCtx &C, int kernel, bool end)
+{
+    if (C.timeline == nullptr || threadIdx.x != 0) return;
+    uint32_t w = *((volatile const uint32_t *)C.wave);
+    if (w >= C.timeline_waves) return;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    unsigned long long *slot = C.timeline + ((size_t)w * 16 + (size_t)kernel) * 2;
+    if (end) atomicMax(slot + 1, t);
+    else atomicMin(slot, t);
+}
+
 __device__ __forceinline__ void consumer_done(const DevCtx &C, int q, int q2 = -1)
 {
     __syncthreads();
@@ -145,12 +165,17 @@ __device__ bool make_primary(const DevCtx &C, unsigned long long h, Part &p)
 
 __global__ void k_source(const __grid_constant__ DevCtx C, const SchedState *st)
 {
+    timeline_mark(C, TL_SOURCE, false);
     unsigned long long h0 = st->h0, h1 = st->h1;
     unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     for (unsigned long long h = h0 + blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; h < h1; h += stride) {
         Part p;
         if (!make_primary(C, h, p)) { atomicOr(C.err, GX_ERR_SOURCE); continue; }
         push(C, p.charge == 0 ? ST_PHOTON : ST_ELECTRON, p);
+    }
+    if (C.timeline) {
+        __syncthreads();
+        timeline_mark(C, TL_SOURCE, true);
     }
 }
 
@@ -212,6 +237,8 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     constexpr int base = ELEC ? GX_Q_ECONT : GX_Q_PCONT;
     constexpr int cls = G - GX_GEOM_JAWS;                // 0 jaws, 1 MLC, 2 phantom
     constexpr bool FIRST = (G == GX_GEOM_PHANTOM);        // takes the new particles
+    constexpr int tl = (ELEC ? TL_ELECTRON : TL_PHOTON) + cls;
+    timeline_mark(C, tl, false);
     const uint32_t par = *C.wave & 1u;
     const int qc_in = base + 2 * cls + (int)par, qc_out = base + 2 * cls + (int)(par ^ 1u);
     const int hq = FIRST ? Q : qc_in;
@@ -258,6 +285,7 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     if (cls < 2) block_stat_add(C, GX_NSTAGE + 2 + 2 * (ELEC ? 1 : 0) + cls, steps);
     if (FIRST) consumer_done(C, Q, qc_in);
     else consumer_done(C, qc_in);
+    timeline_mark(C, tl, true);
 }
 
 __global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_jaws(const __grid_constant__ DevCtx C)
@@ -306,6 +334,8 @@ __device__ __forceinline__ void run_interaction(const DevCtx &C, const Part &p, 
 template <int Q>
 __global__ void __launch_bounds__(256) k_interact(const __grid_constant__ DevCtx C)
 {
+    constexpr int tl = Q < ST_ELECTRON ? TL_PINT + (Q - ST_COMPTON) : TL_EINT + (Q - ST_MOLLER);
+    timeline_mark(C, tl, false);
     const uint32_t n = queue_len(C, Q);
     unsigned long long taken = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -319,6 +349,7 @@ __global__ void __launch_bounds__(256) k_interact(const __grid_constant__ DevCtx
     }
     block_stat_add(C, Q, taken);
     consumer_done(C, Q);
+    timeline_mark(C, tl, true);
 }
 
 // ---- plain form: per-thread pops, one stage per launch ---------------------

@@ -138,7 +138,7 @@ def optimize_weights(model: BeamletModel, w0, target, organ, iterations=20, lr=0
         w.grad = None
         loss = objective(beamlet_dose(w, model), target, organ, prescription, limit)
         loss.backward()
-        history.append(float(loss))
+        history.append(float(loss.detach()))
         with torch.no_grad():
             g = w.grad
             step = lr * float(w.abs().mean()) / max(float(g.abs().max()), 1e-30)
@@ -163,7 +163,7 @@ def optimize_weights_batch(models, w0s, targets, organs, iterations=20, lr=0.05,
             dt = torch.from_numpy(d).requires_grad_(True)
             loss = objective(dt, targets[k], organs[k], prescription, limit)
             loss.backward()
-            hist[k].append(float(loss))
+            hist[k].append(float(loss.detach()))
             g = m.vjp(dt.grad.numpy())
             step = lr * float(np.abs(ws[k]).mean()) / max(float(np.abs(g).max()), 1e-30)
             ws[k] = np.maximum(ws[k] - step * g, 0.0)

@@ -18,7 +18,7 @@ STATUS = {0: "GEGS_OK", 1: "GEGS_ERR_ARG", 2: "GEGS_ERR_CUDA", 3: "GEGS_ERR_QUEU
           5: "GEGS_ERR_NOMEM", 6: "GEGS_ERR_STEP_BUDGET", 7: "GEGS_ERR_SOURCE"}
 MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 
-EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
+EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_set_timeline", "gegs_get_timeline", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
            "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_set_tally", "gegs_get_dose", "gegs_get_stats",
            "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version"]
 
@@ -77,6 +77,8 @@ def load_library(path=None):
     L.gegs_get_stats.argtypes = [vp, C.POINTER(RunStats)]
     L.gegs_tally_device_ptr.argtypes = [vp, C.POINTER(vp)]
     L.gegs_set_trace.argtypes = [vp, C.c_uint32]
+    L.gegs_set_timeline.argtypes = [vp, C.c_uint32]
+    L.gegs_get_timeline.argtypes = [vp, vp, C.c_uint32]
     L.gegs_get_trace.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_uint32)]
     for f in ("gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field"):
         getattr(L, f).restype = C.c_size_t
@@ -171,6 +173,22 @@ class Engine:
     def tally(self) -> np.ndarray:
         out = np.zeros(self.nvox, np.int64)
         self._check(self.L.gegs_get_tally(self.h, out.ctypes.data, self.nvox))
+        return out
+
+    TIMELINE_KERNELS = ["source", "photon_jaws", "photon_mlc", "photon", "compton", "photo", "rayleigh", "pair",
+                        "electron_jaws", "electron_mlc", "electron", "moller", "brems", "bhabha", "annih", "-"]
+
+    def set_timeline(self, max_waves: int):
+        """Record the wave timeline of the following runs (0: off)."""
+        self._check(self.L.gegs_set_timeline(self.h, int(max_waves)))
+        self._timeline_waves = int(max_waves)
+
+    def timeline(self) -> np.ndarray:
+        """[waves, 16, 2] start / end stamps (ns) of the last run; see gegs.h."""
+        n = getattr(self, "_timeline_waves", 0)
+        out = np.zeros((n, 16, 2), np.uint64)
+        if n:
+            self._check(self.L.gegs_get_timeline(self.h, out.ctypes.data, n))
         return out
 
     def set_tally(self, tally: np.ndarray):

@@ -4,6 +4,11 @@ one by one), printing one JSON line with the step counts and per-kernel device
 time. Used as the profiled command for the kernel summaries:
 
     python -m gegs_b200.profile_case --histories 1000000 --batch 524288
+
+With --timeline it runs the persistent form instead (one CUDA graph) and
+prints the wave timeline summary: per phase and per kernel the device time
+summed over waves, from the first-block start and last-block end stamps that
+every kernel writes per wave (gegs_set_timeline).
 """
 from __future__ import annotations
 
@@ -14,19 +19,25 @@ import json
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--histories", type=int, default=1_000_000)
-    ap.add_argument("--batch", type=int, default=524288)
+    ap.add_argument("--batch", type=int, default=524288, help="in-flight batch (0: sized to the run)")
     ap.add_argument("--nphsp", type=int, default=2_000_000)
     ap.add_argument("--dims", default="256,256,120")
+    ap.add_argument("--timeline", action="store_true", help="persistent form with the wave timeline")
+    ap.add_argument("--plan-histories", type=int, default=0, help="histories of the plan (fields split them; 0: --histories)")
+    ap.add_argument("--first", type=int, default=0, help="first history of the run")
     args = ap.parse_args()
     from . import build as B
     B.build()
     from . import workloads as W
     from .engine import MODE_TIMED, Engine
     dims = tuple(int(x) for x in args.dims.split(","))
-    job = W.config3(histories=max(args.histories, 1), nphsp=args.nphsp, dims=dims)
+    job = W.config3(histories=max(args.plan_histories or args.histories, 1), nphsp=args.nphsp, dims=dims)
     eng = Engine(0)
     eng.set_physics(job.physics)
     eng.set_scene(job.scene())
+    if args.timeline:
+        print(json.dumps(timeline_summary(eng, args, dims)))
+        return
     st = eng.run(0, args.histories, mode=MODE_TIMED, batch=args.batch)
     kinds = ["photon", "compton", "photo", "rayleigh", "pair", "electron", "moller", "brems", "bhabha", "annih",
              "source", "planner", "photon_jaws", "electron_jaws", "photon_mlc", "electron_mlc"]
@@ -39,6 +50,39 @@ def main():
         "processed": dict(zip(kinds[:10], st["processed"])),
         "stage_ms": dict(zip(kinds, st["stage_ms"])), "stage_launches": dict(zip(kinds, st["stage_launches"])),
         "error_bits": st["error_bits"]}))
+
+
+def timeline_summary(eng, args, dims):
+    import numpy as np
+    eng.run(args.first, args.first + min(args.histories, 1_000_000), batch=args.batch)   # graph and queues
+    eng.set_timeline(1 << 14)
+    st = eng.run(args.first, args.first + args.histories, batch=args.batch)
+    tl = eng.timeline()[:st["waves"]].astype(np.float64)
+    ran = tl[:, :, 1] > 0
+    t0 = np.min(np.where(ran, tl[:, :, 0], np.inf))
+    s = np.where(ran, (tl[:, :, 0] - t0) / 1e6, np.nan)
+    e = np.where(ran, (tl[:, :, 1] - t0) / 1e6, np.nan)
+    names = eng.TIMELINE_KERNELS
+    groups = {"source": [0], "photon transport": [1, 2, 3], "photon interactions": [4, 5, 6, 7],
+              "electron transport": [8, 9, 10], "electron interactions": [11, 12, 13, 14]}
+    with np.errstate(all="ignore"):
+        span = lambda g: np.nan_to_num(np.nanmax(e[:, g], axis=1) - np.nanmin(s[:, g], axis=1))
+        phases = {k: float(span(g).sum()) for k, g in groups.items()}
+        dur = np.nan_to_num(e - s)
+    kern = {names[k]: float(dur[:, k].sum()) for k in range(15)}
+    # waves whose photon phase is a photon-jaws launch well past the other kernels of the run
+    pj = dur[:, 1]
+    others = np.max(np.delete(dur, [1, 15], axis=1), axis=1)
+    lone = (pj > 0.5) & (pj > 2 * others)
+    return {"workload": f"C3 CT head {dims[0]}x{dims[1]}x{dims[2]}, 5 fields, persistent form",
+            "histories": args.histories, "first": args.first, "batch": args.batch or "auto",
+            "device_ms": st["device_ms"], "waves": st["waves"],
+            "phase_ms": {k: round(v, 1) for k, v in phases.items()},
+            "kernel_ms": {k: round(v, 1) for k, v in kern.items()},
+            "serial_overlap": "kernel sums exceed phase spans where kernels of a phase overlap",
+            "lone_photon_jaws_waves": int(lone.sum()),
+            "lone_photon_jaws_ms": round(float(pj[lone].sum()), 1),
+            "longest_photon_jaws_ms": [round(float(x), 2) for x in np.sort(pj)[::-1][:5]]}
 
 
 if __name__ == "__main__":
