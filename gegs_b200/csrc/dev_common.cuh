@@ -135,6 +135,8 @@ struct DevCtx {
     uint32_t *trace_n;
     uint32_t trace_cap;
     const uint32_t *wave;           // wave counter (parity selects the continuation buffers)
+    uint32_t *photon_done;          // photon MLC and phantom consumers finished in this wave
+    uint32_t overlap;               // 1: a phase's class consumers run as concurrent graph branches
     uint32_t photon_budget, electron_budget;   // steps per particle per launch before continuation
     unsigned long long *timeline;   // [timeline_waves][16][2] first start / last end (ns) per kernel; null: off
     uint32_t timeline_waves;

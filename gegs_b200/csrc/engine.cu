@@ -395,6 +395,8 @@ static void fill_queue_ctx(gegs_engine *e)
     Q.head = e->d_qmeta + GX_NQ;
     Q.done = e->d_qmeta + 2 * GX_NQ;
     e->ctx.wave = &e->d_sched->waves;
+    e->ctx.photon_done = &e->d_sched->photon_done;
+    e->ctx.overlap = 1u;
 }
 
 // One wave of the persistent form, as captured into the graph body. Kernels
@@ -548,7 +550,8 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
             cudaEventElapsedTime(&t, evs[30], evs[31]);
             acc[11] += t; nl[11]++;
             if (!hsr.pending) break;
-            const DevCtx &C = e->ctx;
+            DevCtx C = e->ctx;
+            C.overlap = 0u;             // one kernel at a time
             cudaStream_t s = e->stream;
             // codes 12 / 13: photon / electron consumers of the jaws, 14 / 15: of the MLC
             int slot[15] = {10, 12, 14, ST_PHOTON, ST_COMPTON, ST_PHOTO, ST_RAYLEIGH, ST_PAIR, 13, 15, ST_ELECTRON,
@@ -868,6 +871,8 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
     c.err = err;
     c.stats = stats;
     c.wave = &sched->waves;
+    c.photon_done = &sched->photon_done;
+    c.overlap = 0u;                 // one kernel at a time
     c.timeline = nullptr;
     c.timeline_waves = 0;
     c.trace = nullptr;

@@ -23,6 +23,7 @@ struct SchedState {
     unsigned long long h0, h1;        // histories injected by the current wave
     uint32_t batch, waves, max_waves, pending;
     uint32_t refill_below;
+    uint32_t photon_done;             // photon MLC and phantom consumers finished in this wave
 };
 
 // ---- wave timeline (tracing; off unless DevCtx::timeline is set) ------------
@@ -45,7 +46,7 @@ __device__ __forceinline__ void timeline_mark(const DevCtx &C, int kernel, bool 
     else atomicMin(slot, t);
 }
 
-__device__ __forceinline__ void consumer_done(const DevCtx &C, int q, int q2 = -1)
+__device__ __forceinline__ void consumer_done(const DevCtx &C, int q, int q2 = -1, uint32_t *finished = nullptr)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -57,6 +58,7 @@ __device__ __forceinline__ void consumer_done(const DevCtx &C, int q, int q2 = -
             C.q.done[q] = 0;
             if (q2 >= 0) C.q.count[q2] = 0;
             __threadfence();
+            if (finished) atomicAdd(finished, 1u);
         }
     }
 }
@@ -249,6 +251,14 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     // steps; electrons take 2x theirs in the phantom
     const uint32_t budget = ELEC ? (cls < 2 ? C.electron_budget : 2u * C.electron_budget)
                                  : (cls < 2 ? 8u * C.photon_budget : C.photon_budget);
+    // A jaws photon takes a handful of steps, except the rare one that runs
+    // almost parallel to a jaw face in tens of thousands of tiny steps. Past
+    // its budget such a photon keeps stepping while the other photon consumers
+    // of the wave are still running (up to 64 budgets), so that its long track
+    // advances with the bulk of the work instead of one budget per wave in the
+    // run's tail. Only when the phase's kernels run concurrently (C.overlap).
+    constexpr bool JAWS_PHOTON = !ELEC && G == GX_GEOM_JAWS;
+    const volatile uint32_t *others_done = C.photon_done;
     Part p;
     Rng r;
     EState s;
@@ -271,7 +281,9 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
                 rng_window(C, r);
                 bool done = ELEC ? electron_step<G>(C, p, r, s) : photon_step<G>(C, p, r);
                 if (done) active = false;
-                else if (++nst >= budget) {
+                else if (++nst >= budget &&
+                         (!JAWS_PHOTON || !C.overlap || nst >= 64u * budget ||
+                          (((nst - budget) & 15u) == 0u && *others_done >= 2u))) {
                     if (ELEC) { EStatePk k = pack_estate(s); push_cont(C, qc_out, p, r, &k); }
                     else push_cont(C, qc_out, p, r, nullptr);
                     active = false;
@@ -283,8 +295,9 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     block_stat_add(C, GX_NSTAGE + (ELEC ? 1 : 0), steps);
     // steps in the jaws and the MLC (slots 12-15; the phantom's are the rest)
     if (cls < 2) block_stat_add(C, GX_NSTAGE + 2 + 2 * (ELEC ? 1 : 0) + cls, steps);
-    if (FIRST) consumer_done(C, Q, qc_in);
-    else consumer_done(C, qc_in);
+    uint32_t *fin = (!ELEC && G != GX_GEOM_JAWS) ? C.photon_done : nullptr;
+    if (FIRST) consumer_done(C, Q, qc_in, fin);
+    else consumer_done(C, qc_in, -1, fin);
     timeline_mark(C, tl, true);
 }
 
@@ -410,6 +423,7 @@ __device__ __forceinline__ uint32_t plan_wave(const DevCtx &C, SchedState *st)
     st->h1 = st->next + inject;
     st->next += inject;
     st->waves++;
+    st->photon_done = 0u;
     uint32_t pending = (inflight > 0 || inject > 0 || st->next < st->end) ? 1u : 0u;
     if (pending && st->waves >= st->max_waves) {
         atomicOr(C.err, GX_ERR_STEP_BUDGET);
