@@ -244,8 +244,14 @@ __device__ __forceinline__ void e_discard_below_cut(const DevCtx &C, Part &p, co
 
 // One iteration of the ELECTR loop.  Returns true when the particle has left
 // the electron stage.
-template <int G = GX_GEOM_ALL>
-__device__ bool electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
+// Returns 0 while the particle stays in the electron stage, 1 when it has
+// left it, and (DEFER only) 2 when the step needs howfar: the caller then
+// re-queues the particle as it stood at the start of the step (howfar is the
+// first thing in the step that changes the particle; the step state and the
+// random counter are restored by the caller), and the step runs again, whole,
+// in a pass whose warps hold only such particles.
+template <int G = GX_GEOM_ALL, bool DEFER = false>
+__device__ int electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
 {
     const gegs_physics *P = C.P;
     const float rm = P->rm, prm = P->prm, rmt2 = P->rmt2, rmsq = P->rmsq;
@@ -392,6 +398,7 @@ __device__ bool electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
     int idisc = 0;
     float ustep0 = ustep;
     if (callhowfar || p.wt <= 0.0f) {
+        if (DEFER) return 2;
         bool ok;
         irnew = howfar_g<G>(C, p, ustep, ok);
         if (!ok) { atomicOr(C.err, GX_ERR_MODULE); return true; }

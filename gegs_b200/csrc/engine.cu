@@ -15,7 +15,8 @@ namespace {
 // queue capacity per history in flight, per stage
 constexpr float kCapFactor[GX_NQ] = {6.f, 3.f, 3.f, 3.f, 3.f, 6.f, 3.f, 3.f, 3.f, 3.f,   // stages
                                      2.f, 2.f, 2.f, 2.f, 3.f, 3.f,                        // photon continuations
-                                     2.f, 2.f, 2.f, 2.f, 3.f, 3.f};
+                                     2.f, 2.f, 2.f, 2.f, 3.f, 3.f,
+                                     3.f};                                                // MLC electrons near a boundary
 
 constexpr unsigned long long cap_factor_sum()
 {
@@ -433,6 +434,7 @@ static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
     fork(2);
     k_electron_jaws<<<grid, threads, 0, a[0]>>>(C);
     k_electron_mlc<<<grid, threads, 0, a[1]>>>(C);
+    k_electron_mlc_near<<<grid, threads, 0, a[1]>>>(C);
     k_electron<<<grid, threads, 0, s>>>(C);
     join(2);
     fork(3);
@@ -563,7 +565,10 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
                 case 12: k_photon_jaws<<<grid, threads, 0, s>>>(C); break;
                 case 13: k_electron_jaws<<<grid, threads, 0, s>>>(C); break;
                 case 14: k_photon_mlc<<<grid, threads, 0, s>>>(C); break;
-                case 15: k_electron_mlc<<<grid, threads, 0, s>>>(C); break;
+                case 15:
+                    k_electron_mlc<<<grid, threads, 0, s>>>(C);
+                    k_electron_mlc_near<<<grid, threads, 0, s>>>(C);
+                    break;
                 case ST_PHOTON: k_photon<<<grid, threads, 0, s>>>(C); break;
                 case ST_COMPTON: k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(C); break;
                 case ST_PHOTO: k_interact<ST_PHOTO><<<grid, threads, 0, s>>>(C); break;
@@ -908,6 +913,7 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
             k_interact<ST_PAIR><<<grid, threads, 0, s>>>(c);
             k_electron_jaws<<<grid, threads, 0, s>>>(c);
             k_electron_mlc<<<grid, threads, 0, s>>>(c);
+            k_electron_mlc_near<<<grid, threads, 0, s>>>(c);
             k_electron<<<grid, threads, 0, s>>>(c);
             k_interact<ST_MOLLER><<<grid, threads, 0, s>>>(c);
             k_interact<ST_BREMS><<<grid, threads, 0, s>>>(c);

@@ -32,7 +32,7 @@ struct SchedState {
 // Bhabha, annihilation. Each block's thread 0 lowers the kernel's start stamp
 // of this wave when the block begins and raises its end stamp once the block
 // is done (after the block's barrier).
-enum : int { TL_SOURCE = 0, TL_PHOTON = 1, TL_PINT = 4, TL_ELECTRON = 8, TL_EINT = 11 };
+enum : int { TL_SOURCE = 0, TL_PHOTON = 1, TL_PINT = 4, TL_ELECTRON = 8, TL_EINT = 11, TL_ENEAR = 15 };
 
 __device__ __forceinline__ void timeline_mark(const DevCtx &C, int kernel, bool end)
 {
@@ -232,17 +232,25 @@ __device__ __forceinline__ bool refill(const DevCtx &C, int hq, uint32_t n_cont,
 // outside the class, or one whose step budget for this launch is spent, is
 // re-queued with its state for the next wave (into its class's continuation
 // queue), so the tally does not depend on where a track is split.
-template <bool ELEC, int G>
+//
+// MLC electrons run in two passes. The first hands every step that needs a
+// boundary search (howfar_mlc, the costliest routine of the class, wanted by
+// few lanes of a warp at a time) to the near-boundary queue, as the step stood
+// at its start; the second (NEAR) runs those steps again, whole, and carries
+// its particles on with howfar inline, so that its warps search boundaries
+// with most lanes at once.
+template <bool ELEC, int G, bool NEAR = false>
 __device__ __forceinline__ void transport_consumer(const DevCtx &C)
 {
     constexpr int Q = ELEC ? ST_ELECTRON : ST_PHOTON;
     constexpr int base = ELEC ? GX_Q_ECONT : GX_Q_PCONT;
     constexpr int cls = G - GX_GEOM_JAWS;                // 0 jaws, 1 MLC, 2 phantom
     constexpr bool FIRST = (G == GX_GEOM_PHANTOM);        // takes the new particles
-    constexpr int tl = (ELEC ? TL_ELECTRON : TL_PHOTON) + cls;
+    constexpr bool DEFER = ELEC && G == GX_GEOM_MLC && !NEAR;
+    constexpr int tl = NEAR ? TL_ENEAR : (ELEC ? TL_ELECTRON : TL_PHOTON) + cls;
     timeline_mark(C, tl, false);
     const uint32_t par = *C.wave & 1u;
-    const int qc_in = base + 2 * cls + (int)par, qc_out = base + 2 * cls + (int)(par ^ 1u);
+    const int qc_in = NEAR ? GX_Q_ENEAR : base + 2 * cls + (int)par, qc_out = base + 2 * cls + (int)(par ^ 1u);
     const int hq = FIRST ? Q : qc_in;
     const uint32_t n_cont = queue_len(C, qc_in);
     const uint32_t n = n_cont + (FIRST ? queue_len(C, Q) : 0u);
@@ -279,7 +287,19 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
             } else {
                 steps++;
                 rng_window(C, r);
-                bool done = ELEC ? electron_step<G>(C, p, r, s) : photon_step<G>(C, p, r);
+                bool done;
+                if (DEFER) {
+                    const uint32_t ctr0 = r.ctr;
+                    const EState s0 = s;
+                    const int code = electron_step<G, true>(C, p, r, s);
+                    if (code == 2) {
+                        r.ctr = ctr0;
+                        EStatePk k = pack_estate(s0);
+                        push_cont(C, GX_Q_ENEAR, p, r, &k);
+                        steps--;                      // the step runs in the near-boundary pass
+                    }
+                    done = code != 0;                 // leaves this pass either way
+                } else done = ELEC ? electron_step<G>(C, p, r, s) != 0 : photon_step<G>(C, p, r);
                 if (done) active = false;
                 else if (++nst >= budget &&
                          (!JAWS_PHOTON || !C.overlap || nst >= 64u * budget ||
@@ -324,6 +344,11 @@ __global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_jaws(c
 __global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_mlc(const __grid_constant__ DevCtx C)
 {
     transport_consumer<true, GX_GEOM_MLC>(C);
+}
+
+__global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_mlc_near(const __grid_constant__ DevCtx C)
+{
+    transport_consumer<true, GX_GEOM_MLC, true>(C);
 }
 
 __global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron(const __grid_constant__ DevCtx C)
