@@ -44,15 +44,15 @@ static_assert(sizeof(gegs_field) % 16 == 0, "field record size");
 // continuation queues for each geometry class in beam order (0 jaws, 1 MLC,
 // 2 phantom): photons 10..15, electrons 16..21 (pair = type base + 2 * class).
 // The step-budgeted consumers re-queue into them; electron continuations carry
-// their step state (estate[qid - GX_Q_ECONT]). Queue 22 holds the MLC electron
-// steps that need a boundary search (howfar), as they stood at their start,
-// for the near-boundary pass of the same wave.
+// their step state (estate[qid - GX_Q_ECONT]). Queues 22 (jaws) and 23 (MLC)
+// hold the electron steps that need a boundary search (howfar), as they stood
+// at their start, for the near-boundary pass of the same wave.
 #define GX_NCLASS 3
 #define GX_Q_PCONT 10
 #define GX_Q_ECONT 16
 #define GX_Q_ENEAR 22
-#define GX_NQ 23
-#define GX_NESTATE 7
+#define GX_NQ 24
+#define GX_NESTATE 8
 #define GX_LOOP_CAP 1000
 #define GX_EPSGMFP 1.e-5f
 #define GX_EPSEMFP 1.e-5f

@@ -16,7 +16,7 @@ namespace {
 constexpr float kCapFactor[GX_NQ] = {6.f, 3.f, 3.f, 3.f, 3.f, 6.f, 3.f, 3.f, 3.f, 3.f,   // stages
                                      2.f, 2.f, 2.f, 2.f, 3.f, 3.f,                        // photon continuations
                                      2.f, 2.f, 2.f, 2.f, 3.f, 3.f,
-                                     3.f};                                                // MLC electrons near a boundary
+                                     3.f, 3.f};                                           // jaws / MLC electrons near a boundary
 
 constexpr unsigned long long cap_factor_sum()
 {
@@ -433,6 +433,7 @@ static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
     join(3);
     fork(2);
     k_electron_jaws<<<grid, threads, 0, a[0]>>>(C);
+    k_electron_jaws_near<<<grid, threads, 0, a[0]>>>(C);
     k_electron_mlc<<<grid, threads, 0, a[1]>>>(C);
     k_electron_mlc_near<<<grid, threads, 0, a[1]>>>(C);
     k_electron<<<grid, threads, 0, s>>>(C);
@@ -563,7 +564,10 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
                 switch (slot[k]) {
                 case 10: k_source<<<grid, threads, 0, s>>>(C, e->d_sched); break;
                 case 12: k_photon_jaws<<<grid, threads, 0, s>>>(C); break;
-                case 13: k_electron_jaws<<<grid, threads, 0, s>>>(C); break;
+                case 13:
+                    k_electron_jaws<<<grid, threads, 0, s>>>(C);
+                    k_electron_jaws_near<<<grid, threads, 0, s>>>(C);
+                    break;
                 case 14: k_photon_mlc<<<grid, threads, 0, s>>>(C); break;
                 case 15:
                     k_electron_mlc<<<grid, threads, 0, s>>>(C);
@@ -912,6 +916,7 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
             k_interact<ST_RAYLEIGH><<<grid, threads, 0, s>>>(c);
             k_interact<ST_PAIR><<<grid, threads, 0, s>>>(c);
             k_electron_jaws<<<grid, threads, 0, s>>>(c);
+            k_electron_jaws_near<<<grid, threads, 0, s>>>(c);
             k_electron_mlc<<<grid, threads, 0, s>>>(c);
             k_electron_mlc_near<<<grid, threads, 0, s>>>(c);
             k_electron<<<grid, threads, 0, s>>>(c);

@@ -233,12 +233,12 @@ __device__ __forceinline__ bool refill(const DevCtx &C, int hq, uint32_t n_cont,
 // re-queued with its state for the next wave (into its class's continuation
 // queue), so the tally does not depend on where a track is split.
 //
-// MLC electrons run in two passes. The first hands every step that needs a
-// boundary search (howfar_mlc, the costliest routine of the class, wanted by
-// few lanes of a warp at a time) to the near-boundary queue, as the step stood
-// at its start; the second (NEAR) runs those steps again, whole, and carries
-// its particles on with howfar inline, so that its warps search boundaries
-// with most lanes at once.
+// Electrons in the jaws and the MLC run in two passes. The first hands every
+// step that needs a boundary search (howfar, the costliest routine of these
+// classes, wanted by few lanes of a warp at a time) to its class's
+// near-boundary queue, as the step stood at its start; the second (NEAR) runs
+// those steps again, whole, and carries its particles on with howfar inline,
+// so that its warps search boundaries with most lanes at once.
 template <bool ELEC, int G, bool NEAR = false>
 __device__ __forceinline__ void transport_consumer(const DevCtx &C)
 {
@@ -246,11 +246,11 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     constexpr int base = ELEC ? GX_Q_ECONT : GX_Q_PCONT;
     constexpr int cls = G - GX_GEOM_JAWS;                // 0 jaws, 1 MLC, 2 phantom
     constexpr bool FIRST = (G == GX_GEOM_PHANTOM);        // takes the new particles
-    constexpr bool DEFER = ELEC && G == GX_GEOM_MLC && !NEAR;
+    constexpr bool DEFER = ELEC && (G == GX_GEOM_JAWS || G == GX_GEOM_MLC) && !NEAR;
     constexpr int tl = NEAR ? TL_ENEAR : (ELEC ? TL_ELECTRON : TL_PHOTON) + cls;
     timeline_mark(C, tl, false);
     const uint32_t par = *C.wave & 1u;
-    const int qc_in = NEAR ? GX_Q_ENEAR : base + 2 * cls + (int)par, qc_out = base + 2 * cls + (int)(par ^ 1u);
+    const int qc_in = NEAR ? GX_Q_ENEAR + cls : base + 2 * cls + (int)par, qc_out = base + 2 * cls + (int)(par ^ 1u);
     const int hq = FIRST ? Q : qc_in;
     const uint32_t n_cont = queue_len(C, qc_in);
     const uint32_t n = n_cont + (FIRST ? queue_len(C, Q) : 0u);
@@ -295,7 +295,7 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
                     if (code == 2) {
                         r.ctr = ctr0;
                         EStatePk k = pack_estate(s0);
-                        push_cont(C, GX_Q_ENEAR, p, r, &k);
+                        push_cont(C, GX_Q_ENEAR + cls, p, r, &k);
                         steps--;                      // the step runs in the near-boundary pass
                     }
                     done = code != 0;                 // leaves this pass either way
@@ -344,6 +344,11 @@ __global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_jaws(c
 __global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_mlc(const __grid_constant__ DevCtx C)
 {
     transport_consumer<true, GX_GEOM_MLC>(C);
+}
+
+__global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_jaws_near(const __grid_constant__ DevCtx C)
+{
+    transport_consumer<true, GX_GEOM_JAWS, true>(C);
 }
 
 __global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_mlc_near(const __grid_constant__ DevCtx C)

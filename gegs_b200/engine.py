@@ -177,7 +177,7 @@ class Engine:
 
     TIMELINE_KERNELS = ["source", "photon_jaws", "photon_mlc", "photon", "compton", "photo", "rayleigh", "pair",
                         "electron_jaws", "electron_mlc", "electron", "moller", "brems", "bhabha", "annih",
-                        "electron_mlc_near"]
+                        "electron_near"]
 
     def set_timeline(self, max_waves: int):
         """Record the wave timeline of the following runs (0: off)."""

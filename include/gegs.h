@@ -183,8 +183,8 @@ gegs_status gegs_tally_device_ptr(gegs_engine *e, void **out);
  * kernel the first block's start and the last block's end (%globaltimer, ns)
  * in [wave][kernel][2]. Kernels: 0 source; 1-3 photon jaws, MLC, phantom;
  * 4-7 Compton, photo, Rayleigh, pair; 8-10 electron jaws, MLC, phantom;
- * 11-14 Moller, brems, Bhabha, annihilation; 15 the MLC electrons' near-boundary
- * pass. A kernel that did not
+ * 11-14 Moller, brems, Bhabha, annihilation; 15 the near-boundary passes of
+ * the jaws and MLC electrons (together). A kernel that did not
  * run in a wave keeps start = UINT64_MAX, end = 0. 0 turns it off. */
 gegs_status gegs_set_timeline(gegs_engine *e, uint32_t max_waves);
 gegs_status gegs_get_timeline(gegs_engine *e, uint64_t *out, uint32_t max_waves);
