@@ -225,6 +225,10 @@ __device__ __forceinline__ bool refill(const DevCtx &C, int hq, uint32_t n_cont,
 #ifndef GX_ELECTRON_MIN_BLOCKS
 #define GX_ELECTRON_MIN_BLOCKS 3
 #endif
+// the first pass of the jaws and MLC electrons, without howfar, fits 64 registers
+#ifndef GX_EHEAD_MIN_BLOCKS
+#define GX_EHEAD_MIN_BLOCKS 4
+#endif
 
 // Transport consumer for photons (ELEC false) or electrons of one geometry
 // class G. The three class kernels of a particle type run concurrently; the
@@ -336,12 +340,12 @@ __global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon(const __gr
     transport_consumer<false, GX_GEOM_PHANTOM>(C);
 }
 
-__global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_jaws(const __grid_constant__ DevCtx C)
+__global__ void __launch_bounds__(256, GX_EHEAD_MIN_BLOCKS) k_electron_jaws(const __grid_constant__ DevCtx C)
 {
     transport_consumer<true, GX_GEOM_JAWS>(C);
 }
 
-__global__ void __launch_bounds__(256, GX_ELECTRON_MIN_BLOCKS) k_electron_mlc(const __grid_constant__ DevCtx C)
+__global__ void __launch_bounds__(256, GX_EHEAD_MIN_BLOCKS) k_electron_mlc(const __grid_constant__ DevCtx C)
 {
     transport_consumer<true, GX_GEOM_MLC>(C);
 }
