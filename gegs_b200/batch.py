@@ -19,7 +19,7 @@ import numpy as np
 
 from .engine import Engine
 
-QUEUE_BYTES_PER_PARTICLE = 4.5e3      # event queues + electron step state per particle of `batch`
+QUEUE_BYTES_PER_PARTICLE = 5.2e3      # event queues + electron step state per particle of `batch`
 
 
 def choose_options(histories, share_bytes):
