@@ -312,33 +312,56 @@ __device__ uint32_t howfar_mlc(const DevCtx &C, Part &p0, float &t)
     if (!to_new_region) {
         if (p.leafIndex > -60) index = p.leafIndex;
         else index = index_of_leaf(C, p1);
-        if (index >= 0) {
-            dis_xz = ray_intersect_polygon<false>(p1, dir1, C.crossXZ + index * 16, 14, inside_XZ);
-            const float2 *yzp = endnode_of(C, p.field, index);
-            int nv = 17;
-            if (p.bank == 0) { yzp += 2; nv = 30; }
-            else if (p.bank == 2) { yzp += 17; }
-            dis_yz = ray_intersect_polygon<false>(p2, dir2, yzp, nv, inside_YZ);
-            if (dis_yz > dis_xz) {
-                if (dir1.x < 0 && index > 0) index = -index;
-                else if (index < 59) index = -(index + 1);
+        // In a leaf: the ray against the leaf's XZ cross section, then against
+        // its YZ leaf-end outline. In an air gap: against the XZ cross sections
+        // of the leaves the ray walks through, from the nearest, until one is
+        // hit or the walk leaves the limits. One loop serves both, one polygon
+        // per pass, so leaf and gap lanes of a warp intersect together (each
+        // lane keeps the reference's polygons, points and order).
+        if (index > -60) {
+            const bool leaf = index >= 0;
+            const float2 *yzp = nullptr;
+            int nv = 17, sx = 1, sl = 16, i = 0, lp = 0;
+            if (leaf) {
+                yzp = endnode_of(C, p.field, index);
+                if (p.bank == 0) { yzp += 2; nv = 30; }
+                else if (p.bank == 2) { yzp += 17; }
+            } else {
+                if (dir1.x < 0) { sx = -1; sl = -16; if (indexLimit1 > 0) indexLimit1 -= 1; indexLimit2 = -index + 1; }
+                else { indexLimit2 = indexLimit1; indexLimit1 = -index - 1; }
+                i = -index - sx;
+                if (indexLimit1 < 0) indexLimit1 = 0;
+                if (indexLimit2 > 59) indexLimit2 = 59;
+                if (i < 0) i = 0;
+                if (i > 59) i = 59;
+                lp = i * 16;
             }
-        } else if (index > -60) {
-            int sx = 1, sl = 16;
-            if (dir1.x < 0) { sx = -1; sl = -16; if (indexLimit1 > 0) indexLimit1 -= 1; indexLimit2 = -index + 1; }
-            else { indexLimit2 = indexLimit1; indexLimit1 = -index - 1; }
-            int i = -index - sx;
-            if (indexLimit1 < 0) indexLimit1 = 0;
-            if (indexLimit2 > 59) indexLimit2 = 59;
-            if (i < 0) i = 0;
-            if (i > 59) i = 59;
-            int lp = i * 16;
-            do {
-                temp1 = ray_intersect_polygon<false>(p1, dir1, C.crossXZ + lp, 14, inside_XZ);
-                i += sx;
-                lp += sl;
-            } while (i >= indexLimit1 && i <= indexLimit2 && temp1 >= GX_INFI_DIST);
-            if (temp1 < dis_xz) {
+            float leaf_xz = 0.0f, leaf_yz = 0.0f;
+            int ins, pass = 0;
+            bool more = true;
+            while (more) {
+                const bool yz = leaf && pass == 1;
+                const float2 *poly = leaf ? (pass == 0 ? C.crossXZ + index * 16 : yzp) : C.crossXZ + lp;
+                float d = ray_intersect_polygon<false>(yz ? p2 : p1, yz ? dir2 : dir1, poly, yz ? nv : 14, ins);
+                if (leaf) {
+                    if (pass == 0) leaf_xz = d;
+                    else { leaf_yz = d; more = false; }
+                } else {
+                    temp1 = d;
+                    i += sx;
+                    lp += sl;
+                    more = i >= indexLimit1 && i <= indexLimit2 && temp1 >= GX_INFI_DIST;
+                }
+                pass++;
+            }
+            if (leaf) {
+                dis_xz = leaf_xz;
+                dis_yz = leaf_yz;
+                if (dis_yz > dis_xz) {
+                    if (dir1.x < 0 && index > 0) index = -index;
+                    else if (index < 59) index = -(index + 1);
+                }
+            } else if (temp1 < dis_xz) {
                 dis_xz = temp1;
                 index = i - sx;
             } else {
