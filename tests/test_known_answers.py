@@ -7,7 +7,9 @@ reference's missing test data:
   between energy and angle;
 * direction rotations keep unit length and the requested polar angle;
 * the voxel walk of howfar_phantom visits the voxels an exact ray traversal
-  visits, with step lengths adding up to the chord.
+  visits, with step lengths adding up to the chord;
+* the electron and positron range tables are the integral of the inverse
+  stopping power of the same tables (CSDA-range consistency).
 """
 import numpy as np
 import pytest
@@ -118,3 +120,33 @@ def test_voxel_walk_matches_exact_traversal(oracle):
         assert abs(steps[k[0] + 1:k[-1] + 2].sum() - (cross[-1] - cross[0])) < 1e-3
         checked += 1
     assert checked > 100
+
+
+@pytest.mark.parametrize("qel", [0, 1])
+def test_range_table_is_the_integral_of_the_inverse_stopping_power(qel):
+    """range_ep (the CSDA range from the lowest table energy, built as in
+    PhysicsInit.cu:1007-1180 with its second-order bin correction) against a
+    fine numerical integral of dE / (dE/dx) over the same log-linear
+    stopping-power table, for electrons (qel 0) and positrons (qel 1)."""
+    blk = PD.build_block(["H2O700ICRU"])
+    from gegs_b200 import physics_layout as L
+    m = 0
+    ex, ey = (float(v) for v in blk["eke01"][m])
+    dedx = blk["dedx"][qel * L.MXEKE * L.MXMED + m * L.MXEKE: qel * L.MXEKE * L.MXMED + (m + 1) * L.MXEKE].astype(float)
+    e_arr = blk["e_array"][m * L.MXEKE: (m + 1) * L.MXEKE].astype(float)
+    rng = blk["range_ep"][2 * m * L.MXEKE: 2 * (m + 1) * L.MXEKE].reshape(-1, 2)[:, qel].astype(float)
+
+    def stopping(e):
+        le = np.log(e)
+        i = np.clip((ex + ey * le).astype(int), 1, L.MXEKE) - 1
+        return dedx[i, 0] + dedx[i, 1] * le
+
+    checked = 0
+    for k in range(8, L.MXEKE - 1, 9):
+        e = np.exp(np.linspace(np.log(e_arr[0]), np.log(e_arr[k]), 20001))
+        f = 1.0 / stopping(e)
+        integral = float(np.sum((f[1:] + f[:-1]) / 2 * np.diff(e)))
+        assert rng[k] == pytest.approx(integral, rel=2e-3), k
+        checked += 1
+    assert checked >= 10
+    assert (np.diff(rng[:L.MXEKE - 1]) > 0).all()      # a range grows with energy
