@@ -122,6 +122,32 @@ struct QueueSet {
     uint32_t *done;       // [GX_NQ] finished blocks of the running consumer
 };
 
+// Unsigned division by a divisor fixed for the run, as a multiply-high and
+// shifts (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, fig. 4.1): exact for every 32-bit dividend.
+struct FastDiv {
+    uint32_t m, sh, one;
+};
+
+__host__ __device__ inline FastDiv make_fastdiv(uint32_t d)
+{
+    FastDiv f = {0u, 0u, d == 1u ? 1u : 0u};
+    if (d > 1u) {
+        uint32_t l = 0;
+        while ((1ull << l) < d) l++;                     // l = ceil(log2 d), 1..31 here
+        f.m = (uint32_t)((((1ull << 32) * ((1ull << l) - d)) / d) + 1ull);
+        f.sh = l - 1u;
+    }
+    return f;
+}
+
+__device__ __forceinline__ uint32_t fastdiv(const FastDiv &f, uint32_t n)
+{
+    if (f.one) return n;
+    const uint32_t t = __umulhi(f.m, n);
+    return (t + ((n - t) >> 1)) >> f.sh;
+}
+
 // Everything a transport kernel needs; passed by value as a kernel parameter.
 struct DevCtx {
     const gegs_physics *P;
@@ -146,6 +172,7 @@ struct DevCtx {
     QueueSet q;
     uint64_t nphsp;
     int nx, ny, nz, nfields;
+    FastDiv div_nx, div_nxny;       // voxel index decode: / nx, / (nx * ny)
     int change_xyz, hownear_off;
     float sid, iso0, iso1, iso2, z_phsp;
     float mlc_rmax, mlc_zmin, mlc_zthick, mlc_x_start, mlc_x_end, mlc_x_mid_1, mlc_x_mid_2;

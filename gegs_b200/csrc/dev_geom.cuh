@@ -54,9 +54,9 @@ __device__ uint32_t howfar_phantom(const DevCtx &C, const Part &p0, float &t)
     uint32_t region = p0.region;
     if (region >= GX_VAC_AND_OTH) {
         uint32_t ir = region - GX_VAC_AND_OTH;
-        int iz = (int)(ir / (Nx * Ny));
+        int iz = (int)fastdiv(C.div_nxny, ir);
         ir -= (uint32_t)iz * Nx * Ny;
-        int iy = (int)(ir / Nx);
+        int iy = (int)fastdiv(C.div_nx, ir);
         int ix = (int)(ir - (uint32_t)iy * Nx);
         uint32_t inew = region;
         if (p.u > 0.0f) {
@@ -133,9 +133,9 @@ __device__ void hownear_phantom(const DevCtx &C, const Part &p0, float &tperp)
     tperp = GX_INFI_DIST;
     if (p0.region > off - 1u) {
         uint32_t ir = p0.region - off;
-        int iz = (int)(ir / (Nx * Ny));
+        int iz = (int)fastdiv(C.div_nxny, ir);
         ir -= (uint32_t)iz * Nx * Ny;
-        int iy = (int)(ir / Nx);
+        int iy = (int)fastdiv(C.div_nx, ir);
         int ix = (int)(ir - (uint32_t)iy * Nx);
         float tx, ty, tz, tmp;
         tmp = __ldg(&xb[ix + 1]) - p.x; tx = p.x - __ldg(&xb[ix]); if (tmp < tx) tx = tmp;

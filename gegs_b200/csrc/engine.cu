@@ -300,6 +300,8 @@ gegs_status gegs_set_scene(gegs_engine *e, const gegs_scene *S)
     C.err = e->d_err;
     C.stats = e->d_stats;
     C.nx = S->nx; C.ny = S->ny; C.nz = S->nz; C.nfields = S->nfields;
+    C.div_nx = make_fastdiv((uint32_t)S->nx);
+    C.div_nxny = make_fastdiv((uint32_t)S->nx * (uint32_t)S->ny);
     C.change_xyz = S->change_xyz;
     C.hownear_off = S->hownear_region_offset == 6 ? 6 : 5;
     C.sid = S->source_to_isocenter;
