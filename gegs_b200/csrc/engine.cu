@@ -404,9 +404,11 @@ static void fill_queue_ctx(gegs_engine *e)
 
 // One wave of the persistent form, as captured into the graph body. Kernels
 // with no data between them run as parallel branches: the three photon
-// consumers, the four photon interactions, the three electron consumers and
-// the four electron interactions (each reads its own queues; the pushes they
-// share are atomic appends read only by a later phase).
+// consumers, the four photon interactions, the three electron consumers (the
+// jaws and MLC branches each followed by their near-boundary pass, which
+// drains what the first pass queued) and the four electron interactions (each
+// reads its own queues; the pushes they share are atomic appends read only by
+// a later phase).
 static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
 {
     const DevCtx &C = e->ctx;
