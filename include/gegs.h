@@ -116,7 +116,7 @@ gegs_status gegs_wait(gegs_engine *e);
  * gegs_run_noalloc transports histories [hist_begin, hist_end) like gegs_run
  * and adds to the same tally, but it allocates no device memory. Its event
  * queues, scheduler state and counters live in one fixed array compiled into
- * the library (about 25 MB, held on every GPU that loads the library until the
+ * the library (about 28 MB, held on every GPU that loads the library until the
  * process exits). Use it when the caller cannot allocate at run time:
  *   - a planning system or dose server that reserved the GPU's memory when it
  *     started, where a later cudaMalloc of gegs_run's queues (several GB at
