@@ -245,12 +245,13 @@ __device__ __forceinline__ void e_discard_below_cut(const DevCtx &C, Part &p, co
 // One iteration of the ELECTR loop.  Returns true when the particle has left
 // the electron stage.
 // Returns 0 while the particle stays in the electron stage, 1 when it has
-// left it, and (DEFER only) 2 when the step needs howfar: the caller then
+// left it, (DEFER only) 2 when the step needs howfar and (ONLY_NEAR only) 3
+// when it does not, before the step changes the particle: the caller then
 // re-queues the particle as it stood at the start of the step (howfar is the
 // first thing in the step that changes the particle; the step state and the
 // random counter are restored by the caller), and the step runs again, whole,
 // in a pass whose warps hold only such particles.
-template <int G = GX_GEOM_ALL, bool DEFER = false>
+template <int G = GX_GEOM_ALL, bool DEFER = false, bool ONLY_NEAR = false>
 __device__ int electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
 {
     const gegs_physics *P = C.P;
@@ -366,6 +367,7 @@ __device__ int electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
             callmsdist = true;
             de = compute_eloss(P, qel, medium, tustep, range, rhof, eke_val, elke, lelke);
             tvstep = tustep;
+            if (ONLY_NEAR) return 3;
             msdist_pI(C, de, tustep, p, ustep, rd, r);
         } else {
             if (P->exact_bca) {
@@ -392,6 +394,7 @@ __device__ int electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
                 else ustep = tustep * (1.0f - gx_exp(-xi)) / xi;
             }
             callhowfar = !(ustep < tperp);
+            if (ONLY_NEAR && !callhowfar) return 3;
         }
     }
     uint32_t irnew = p.region;

@@ -241,8 +241,10 @@ __device__ __forceinline__ bool refill(const DevCtx &C, int hq, uint32_t n_cont,
 // step that needs a boundary search (howfar, the costliest routine of these
 // classes, wanted by few lanes of a warp at a time) to its class's
 // near-boundary queue, as the step stood at its start; the second (NEAR) runs
-// those steps again, whole, and carries its particles on with howfar inline,
-// so that its warps search boundaries with most lanes at once.
+// those steps again, whole, and carries its particles on while their steps
+// need howfar, so that its warps search boundaries with most lanes at once. A
+// step that does not goes back, as it stood, to the first pass of the next
+// wave.
 template <bool ELEC, int G, bool NEAR = false>
 __device__ __forceinline__ void transport_consumer(const DevCtx &C)
 {
@@ -292,15 +294,18 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
                 steps++;
                 rng_window(C, r);
                 bool done;
-                if (DEFER) {
+                if (DEFER || (ELEC && NEAR)) {
                     const uint32_t ctr0 = r.ctr;
                     const EState s0 = s;
-                    const int code = electron_step<G, true>(C, p, r, s);
-                    if (code == 2) {
+                    const int code = DEFER ? electron_step<G, true, false>(C, p, r, s)
+                                           : electron_step<G, false, true>(C, p, r, s);
+                    if (code >= 2) {
+                        // needs howfar (to the near-boundary pass) or, in that pass, does
+                        // not (back to the first pass of the next wave): re-queued as it stood
                         r.ctr = ctr0;
                         EStatePk k = pack_estate(s0);
-                        push_cont(C, GX_Q_ENEAR + cls, p, r, &k);
-                        steps--;                      // the step runs in the near-boundary pass
+                        push_cont(C, code == 2 ? GX_Q_ENEAR + cls : qc_out, p, r, &k);
+                        steps--;
                     }
                     done = code != 0;                 // leaves this pass either way
                 } else done = ELEC ? electron_step<G>(C, p, r, s) != 0 : photon_step<G>(C, p, r);
