@@ -46,13 +46,17 @@ static_assert(sizeof(gegs_field) % 16 == 0, "field record size");
 // The step-budgeted consumers re-queue into them; electron continuations carry
 // their step state (estate[qid - GX_Q_ECONT]). Queues 22 (jaws) and 23 (MLC)
 // hold the electron steps that need a boundary search (howfar), as they stood
-// at their start, for the near-boundary pass of the same wave.
+// at their start, for the near-boundary pass of the same wave. Queue 24 holds
+// the jaws photons past their step limit, for the long-track kernel that runs
+// beside the electron phase.
 #define GX_NCLASS 3
 #define GX_Q_PCONT 10
 #define GX_Q_ECONT 16
 #define GX_Q_ENEAR 22
-#define GX_NQ 24
+#define GX_Q_PLONG 24
+#define GX_NQ 25
 #define GX_NESTATE 8
+#define GX_TL_KERNELS 32   // wave timeline slots per wave
 #define GX_LOOP_CAP 1000
 #define GX_EPSGMFP 1.e-5f
 #define GX_EPSEMFP 1.e-5f
@@ -165,6 +169,7 @@ struct DevCtx {
     uint32_t trace_cap;
     const uint32_t *wave;           // wave counter (parity selects the continuation buffers)
     uint32_t *photon_done;          // photon MLC and phantom consumers finished in this wave
+    uint32_t *electron_done;        // electron branches (jaws, MLC, phantom) finished in this wave
     uint32_t overlap;               // 1: a phase's class consumers run as concurrent graph branches
     uint32_t photon_budget, electron_budget;   // steps per particle per launch before continuation
     unsigned long long *timeline;   // [timeline_waves][16][2] first start / last end (ns) per kernel; null: off

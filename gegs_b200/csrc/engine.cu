@@ -16,7 +16,8 @@ namespace {
 constexpr float kCapFactor[GX_NQ] = {6.f, 3.f, 3.f, 3.f, 3.f, 6.f, 3.f, 3.f, 3.f, 3.f,   // stages
                                      2.f, 2.f, 2.f, 2.f, 3.f, 3.f,                        // photon continuations
                                      2.f, 2.f, 2.f, 2.f, 3.f, 3.f,
-                                     3.f, 3.f};                                           // jaws / MLC electrons near a boundary
+                                     3.f, 3.f,                                            // jaws / MLC electrons near a boundary
+                                     1.f};                                                // long jaws photon tracks
 
 constexpr unsigned long long cap_factor_sum()
 {
@@ -399,6 +400,7 @@ static void fill_queue_ctx(gegs_engine *e)
     Q.done = e->d_qmeta + 2 * GX_NQ;
     e->ctx.wave = &e->d_sched->waves;
     e->ctx.photon_done = &e->d_sched->photon_done;
+    e->ctx.electron_done = &e->d_sched->electron_done;
     e->ctx.overlap = 1u;
 }
 
@@ -406,9 +408,9 @@ static void fill_queue_ctx(gegs_engine *e)
 // with no data between them run as parallel branches: the three photon
 // consumers, the four photon interactions, the three electron consumers (the
 // jaws and MLC branches each followed by their near-boundary pass, which
-// drains what the first pass queued) and the four electron interactions (each
-// reads its own queues; the pushes they share are atomic appends read only by
-// a later phase).
+// drains what the first pass queued) with the long jaws-photon tracks beside
+// them, and the four electron interactions (each reads its own queues; the
+// pushes they share are atomic appends read only by a later phase).
 static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
 {
     const DevCtx &C = e->ctx;
@@ -435,13 +437,14 @@ static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
     k_interact<ST_RAYLEIGH><<<grid, threads, 0, a[1]>>>(C);
     k_interact<ST_PAIR><<<grid, threads, 0, a[2]>>>(C);
     join(3);
-    fork(2);
+    fork(3);
+    k_photon_jaws_long<<<grid, threads, 0, a[2]>>>(C);
     k_electron_jaws<<<grid, threads, 0, a[0]>>>(C);
     k_electron_jaws_near<<<grid, threads, 0, a[0]>>>(C);
     k_electron_mlc<<<grid, threads, 0, a[1]>>>(C);
     k_electron_mlc_near<<<grid, threads, 0, a[1]>>>(C);
     k_electron<<<grid, threads, 0, s>>>(C);
-    join(2);
+    join(3);
     fork(3);
     k_interact<ST_MOLLER><<<grid, threads, 0, s>>>(C);
     k_interact<ST_BREMS><<<grid, threads, 0, a[0]>>>(C);
@@ -521,7 +524,7 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
     CK(cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 16, e->stream), "stats reset");
     if (e->d_timeline) {
         // start stamps at the maximum, end stamps at 0 (each wave x kernel pair)
-        e->timeline_init.resize((size_t)e->timeline_waves * 32);
+        e->timeline_init.resize((size_t)e->timeline_waves * GX_TL_KERNELS * 2);
         for (size_t i = 0; i < e->timeline_init.size(); i += 2) {
             e->timeline_init[i] = ~0ull;
             e->timeline_init[i + 1] = 0ull;
@@ -739,7 +742,7 @@ extern "C" gegs_status gegs_set_timeline(gegs_engine *e, uint32_t max_waves)
     e->d_timeline = nullptr;
     e->timeline_waves = 0;
     if (max_waves) {
-        CK(cudaMalloc(&e->d_timeline, (size_t)max_waves * 32 * sizeof(unsigned long long)), "timeline");
+        CK(cudaMalloc(&e->d_timeline, (size_t)max_waves * GX_TL_KERNELS * 2 * sizeof(unsigned long long)), "timeline");
         e->timeline_waves = max_waves;
     }
     e->ctx.timeline = e->d_timeline;
@@ -752,7 +755,7 @@ extern "C" gegs_status gegs_get_timeline(gegs_engine *e, uint64_t *out, uint32_t
 {
     if (!e || !out || !e->d_timeline) return GEGS_ERR_ARG;
     uint32_t m = max_waves < e->timeline_waves ? max_waves : e->timeline_waves;
-    CK(cudaMemcpy(out, e->d_timeline, (size_t)m * 32 * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+    CK(cudaMemcpy(out, e->d_timeline, (size_t)m * GX_TL_KERNELS * 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
        "timeline D2H");
     return GEGS_OK;
 }
@@ -885,6 +888,7 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
     c.stats = stats;
     c.wave = &sched->waves;
     c.photon_done = &sched->photon_done;
+    c.electron_done = &sched->electron_done;
     c.overlap = 0u;                 // one kernel at a time
     c.timeline = nullptr;
     c.timeline_waves = 0;

@@ -24,6 +24,7 @@ struct SchedState {
     uint32_t batch, waves, max_waves, pending;
     uint32_t refill_below;
     uint32_t photon_done;             // photon MLC and phantom consumers finished in this wave
+    uint32_t electron_done;           // electron branches finished in this wave
 };
 
 // ---- wave timeline (tracing; off unless DevCtx::timeline is set) ------------
@@ -32,7 +33,7 @@ struct SchedState {
 // Bhabha, annihilation. Each block's thread 0 lowers the kernel's start stamp
 // of this wave when the block begins and raises its end stamp once the block
 // is done (after the block's barrier).
-enum : int { TL_SOURCE = 0, TL_PHOTON = 1, TL_PINT = 4, TL_ELECTRON = 8, TL_EINT = 11, TL_ENEAR = 15 };
+enum : int { TL_SOURCE = 0, TL_PHOTON = 1, TL_PINT = 4, TL_ELECTRON = 8, TL_EINT = 11, TL_ENEAR = 15, TL_PLONG = 16 };
 
 __device__ __forceinline__ void timeline_mark(const DevCtx &C, int kernel, bool end)
 {
@@ -41,7 +42,7 @@ __device__ __forceinline__ void timeline_mark(const DevCtx &C, int kernel, bool 
     if (w >= C.timeline_waves) return;
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    unsigned long long *slot = C.timeline + ((size_t)w * 16 + (size_t)kernel) * 2;
+    unsigned long long *slot = C.timeline + ((size_t)w * GX_TL_KERNELS + (size_t)kernel) * 2;
     if (end) atomicMax(slot + 1, t);
     else atomicMin(slot, t);
 }
@@ -253,10 +254,13 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     constexpr int cls = G - GX_GEOM_JAWS;                // 0 jaws, 1 MLC, 2 phantom
     constexpr bool FIRST = (G == GX_GEOM_PHANTOM);        // takes the new particles
     constexpr bool DEFER = ELEC && (G == GX_GEOM_JAWS || G == GX_GEOM_MLC) && !NEAR;
-    constexpr int tl = NEAR ? TL_ENEAR : (ELEC ? TL_ELECTRON : TL_PHOTON) + cls;
+    // the photon jaws kernel's second form (NEAR): the long tracks, beside the electron phase
+    constexpr bool LONG = !ELEC && G == GX_GEOM_JAWS && NEAR;
+    constexpr int tl = LONG ? TL_PLONG : NEAR ? TL_ENEAR : (ELEC ? TL_ELECTRON : TL_PHOTON) + cls;
     timeline_mark(C, tl, false);
     const uint32_t par = *C.wave & 1u;
-    const int qc_in = NEAR ? GX_Q_ENEAR + cls : base + 2 * cls + (int)par, qc_out = base + 2 * cls + (int)(par ^ 1u);
+    const int qc_in = LONG ? GX_Q_PLONG : NEAR ? GX_Q_ENEAR + cls : base + 2 * cls + (int)par;
+    const int qc_out = base + 2 * cls + (int)(par ^ 1u);
     const int hq = FIRST ? Q : qc_in;
     const uint32_t n_cont = queue_len(C, qc_in);
     const uint32_t n = n_cont + (FIRST ? queue_len(C, Q) : 0u);
@@ -272,7 +276,12 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     // advances with the bulk of the work instead of one budget per wave in the
     // run's tail. Only when the phase's kernels run concurrently (C.overlap).
     constexpr bool JAWS_PHOTON = !ELEC && G == GX_GEOM_JAWS;
-    const volatile uint32_t *others_done = C.photon_done;
+    const volatile uint32_t *others_done = LONG ? C.electron_done : C.photon_done;
+    constexpr uint32_t others = LONG ? 3u : 2u;
+    // in the persistent form, a jaws photon still going when the photon phase
+    // ends moves on to the long-track kernel, which runs beside the electron
+    // phase the same way
+    const int q_limit = (JAWS_PHOTON && !LONG && C.overlap) ? GX_Q_PLONG : qc_out;
     Part p;
     Rng r;
     EState s;
@@ -312,9 +321,9 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
                 if (done) active = false;
                 else if (++nst >= budget &&
                          (!JAWS_PHOTON || !C.overlap || nst >= 64u * budget ||
-                          (((nst - budget) & 15u) == 0u && *others_done >= 2u))) {
+                          (((nst - budget) & 15u) == 0u && *others_done >= others))) {
                     if (ELEC) { EStatePk k = pack_estate(s); push_cont(C, qc_out, p, r, &k); }
-                    else push_cont(C, qc_out, p, r, nullptr);
+                    else push_cont(C, q_limit, p, r, nullptr);
                     active = false;
                 }
             }
@@ -324,7 +333,10 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     block_stat_add(C, GX_NSTAGE + (ELEC ? 1 : 0), steps);
     // steps in the jaws and the MLC (slots 12-15; the phantom's are the rest)
     if (cls < 2) block_stat_add(C, GX_NSTAGE + 2 + 2 * (ELEC ? 1 : 0) + cls, steps);
-    uint32_t *fin = (!ELEC && G != GX_GEOM_JAWS) ? C.photon_done : nullptr;
+    // the last kernel of each photon branch but the jaws (MLC, phantom), and of
+    // each electron branch (jaws and MLC near-boundary passes, phantom)
+    uint32_t *fin = (!ELEC && G != GX_GEOM_JAWS) ? C.photon_done
+                  : (ELEC && (NEAR || G == GX_GEOM_PHANTOM)) ? C.electron_done : nullptr;
     if (FIRST) consumer_done(C, Q, qc_in, fin);
     else consumer_done(C, qc_in, -1, fin);
     timeline_mark(C, tl, true);
@@ -333,6 +345,11 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
 __global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_jaws(const __grid_constant__ DevCtx C)
 {
     transport_consumer<false, GX_GEOM_JAWS>(C);
+}
+
+__global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_jaws_long(const __grid_constant__ DevCtx C)
+{
+    transport_consumer<false, GX_GEOM_JAWS, true>(C);
 }
 
 __global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_mlc(const __grid_constant__ DevCtx C)
@@ -463,6 +480,7 @@ __device__ __forceinline__ uint32_t plan_wave(const DevCtx &C, SchedState *st)
     st->next += inject;
     st->waves++;
     st->photon_done = 0u;
+    st->electron_done = 0u;
     uint32_t pending = (inflight > 0 || inject > 0 || st->next < st->end) ? 1u : 0u;
     if (pending && st->waves >= st->max_waves) {
         atomicOr(C.err, GX_ERR_STEP_BUDGET);

@@ -177,7 +177,8 @@ class Engine:
 
     TIMELINE_KERNELS = ["source", "photon_jaws", "photon_mlc", "photon", "compton", "photo", "rayleigh", "pair",
                         "electron_jaws", "electron_mlc", "electron", "moller", "brems", "bhabha", "annih",
-                        "electron_near"]
+                        "electron_near", "photon_jaws_long"]
+    TIMELINE_SLOTS = 32
 
     def set_timeline(self, max_waves: int):
         """Record the wave timeline of the following runs (0: off)."""
@@ -185,9 +186,9 @@ class Engine:
         self._timeline_waves = int(max_waves)
 
     def timeline(self) -> np.ndarray:
-        """[waves, 16, 2] start / end stamps (ns) of the last run; see gegs.h."""
+        """[waves, 32, 2] start / end stamps (ns) of the last run; see gegs.h."""
         n = getattr(self, "_timeline_waves", 0)
-        out = np.zeros((n, 16, 2), np.uint64)
+        out = np.zeros((n, self.TIMELINE_SLOTS, 2), np.uint64)
         if n:
             self._check(self.L.gegs_get_timeline(self.h, out.ctypes.data, n))
         return out

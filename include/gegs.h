@@ -181,10 +181,11 @@ gegs_status gegs_tally_device_ptr(gegs_engine *e, void **out);
  * launch with events, CUDA_EGS.cu:249-294): with max_waves > 0, every run of
  * the persistent or timed form records for waves 0..max_waves-1 and each
  * kernel the first block's start and the last block's end (%globaltimer, ns)
- * in [wave][kernel][2]. Kernels: 0 source; 1-3 photon jaws, MLC, phantom;
+ * in [wave][32][2]. Kernels: 0 source; 1-3 photon jaws, MLC, phantom;
  * 4-7 Compton, photo, Rayleigh, pair; 8-10 electron jaws, MLC, phantom;
  * 11-14 Moller, brems, Bhabha, annihilation; 15 the near-boundary passes of
- * the jaws and MLC electrons (together). A kernel that did not
+ * the jaws and MLC electrons (together); 16 the long jaws-photon tracks run
+ * beside the electron phase; 17-31 unused. A kernel that did not
  * run in a wave keeps start = UINT64_MAX, end = 0. 0 turns it off. */
 gegs_status gegs_set_timeline(gegs_engine *e, uint32_t max_waves);
 gegs_status gegs_get_timeline(gegs_engine *e, uint64_t *out, uint32_t max_waves);
