@@ -468,7 +468,7 @@ def main():
     # ---- C4: beamlet gradient by replay vs forward and finite differences ---
     grad = c4_gradient(args, eng) if args.c4_histories > 0 else None
     nvox = eng.nvox
-    eng.close()                                    # its event queues (up to ~86 GB) before the C5 engines
+    eng.close()                                    # its event queues (up to ~87 GB) before the C5 engines
     batched = c5_batch(args, local) if args.c5_plans > 0 else None
 
     cpu = None

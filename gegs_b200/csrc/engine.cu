@@ -359,7 +359,7 @@ constexpr unsigned long long kQueueBytesPerParticle =
 // In-flight batch when the caller leaves it at 0: a power of two near half of
 // the run's histories (more particles in flight keep more lanes busy and need
 // fewer waves: on the CT 5-field plan 16M is 7 % faster than 6M), between 64K
-// and 16M (about 86 GB of queues), and within 60 % of the device memory that
+// and 16M (about 87 GB of queues), and within 60 % of the device memory that
 // is free once this engine's current queues are counted as free.
 static uint32_t default_batch(gegs_engine *e, uint64_t histories)
 {

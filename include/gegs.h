@@ -55,8 +55,8 @@ typedef enum gegs_mode {
 typedef struct gegs_run_opts {
     int32_t mode;              /* gegs_mode */
     uint32_t batch;            /* particles kept in flight (0 = a power of two near half the run's histories,
-                                  64K to 16M, within 60 % of free device memory; queue memory ~5.1 KB each,
-                                  ~86 GB at 16M) */
+                                  64K to 16M, within 60 % of free device memory; queue memory ~5.2 KB each,
+                                  ~87 GB at 16M) */
     int32_t blocks_per_sm;     /* 0 = default */
     int32_t threads_per_block; /* 0 = default */
     uint32_t max_waves;        /* safety budget (0 = default) */
