@@ -498,7 +498,9 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
     if (opts) o = *opts;
     uint32_t batch = o.batch ? o.batch : default_batch(e, hist_end - hist_begin);
     int threads = o.threads_per_block ? o.threads_per_block : 256;
-    int bps = o.blocks_per_sm ? o.blocks_per_sm : 4;
+    // 6 blocks per SM: more than the 3-4 that fit at once, so that a block that
+    // finishes early is replaced while a consumer's queue still has work (C3: -0.8 %)
+    int bps = o.blocks_per_sm ? o.blocks_per_sm : 6;
     int grid = e->nsm * bps;
     uint32_t max_waves = o.max_waves ? o.max_waves : 200000u;
     uint32_t pb = (o.step_budget & 0xFFFFu) ? (o.step_budget & 0xFFFFu) : 32u;

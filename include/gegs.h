@@ -57,7 +57,7 @@ typedef struct gegs_run_opts {
     uint32_t batch;            /* particles kept in flight (0 = a power of two near half the run's histories,
                                   64K to 16M, within 60 % of free device memory; queue memory ~5.2 KB each,
                                   ~87 GB at 16M) */
-    int32_t blocks_per_sm;     /* 0 = default */
+    int32_t blocks_per_sm;     /* 0 = default (6: grid = 6 x SM count) */
     int32_t threads_per_block; /* 0 = default */
     uint32_t max_waves;        /* safety budget (0 = default) */
     uint32_t step_budget;      /* steps per particle per launch before it is continued in the next wave:
