@@ -226,6 +226,10 @@ __device__ __forceinline__ bool refill(const DevCtx &C, int hq, uint32_t n_cont,
 #ifndef GX_ELECTRON_MIN_BLOCKS
 #define GX_ELECTRON_MIN_BLOCKS 3
 #endif
+// the MLC photon kernel, the most divergent, runs best with 80 registers (fewer spills)
+#ifndef GX_PMLC_MIN_BLOCKS
+#define GX_PMLC_MIN_BLOCKS 3
+#endif
 // the first pass of the jaws and MLC electrons, without howfar, fits 64 registers
 #ifndef GX_EHEAD_MIN_BLOCKS
 #define GX_EHEAD_MIN_BLOCKS 4
@@ -352,7 +356,7 @@ __global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_jaws_long(
     transport_consumer<false, GX_GEOM_JAWS, true>(C);
 }
 
-__global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_mlc(const __grid_constant__ DevCtx C)
+__global__ void __launch_bounds__(256, GX_PMLC_MIN_BLOCKS) k_photon_mlc(const __grid_constant__ DevCtx C)
 {
     transport_consumer<false, GX_GEOM_MLC>(C);
 }
