@@ -1,7 +1,8 @@
 /* Probes of single oracle routines on controlled inputs, for the project's
  * known-answer tests: the Compton sampler against the analytic Klein-Nishina
- * cross section, direction rotations against orthonormality, and the voxel
- * walk of howfar_phantom against an analytic ray traversal.
+ * cross section, the Moller sampler against the Moller cross section,
+ * direction rotations against orthonormality, and the voxel walk of
+ * howfar_phantom against an analytic ray traversal.
  * Test infrastructure only (see ora_internal.h). */
 #include <stdlib.h>
 #include <string.h>
@@ -54,6 +55,47 @@ int ora_probe_compton(const gegs_physics *P, int medium, uint32_t flags, float e
         cos_out[i] = 2.0f;
         for (size_t k = 0; k < stk.n; k++)
             if (stk.a[k].charge == 0) { e_out[i] = stk.a[k].e; cos_out[i] = stk.a[k].w; }
+    }
+    free(stk.a);
+    return C.error;
+}
+
+/* n Moller events of electrons of kinetic energy `ekin` along +z in one
+ * region of `medium` (cuts of the region at 0, so both electrons leave the
+ * event): per event the kinetic energy of the slower electron over ekin and
+ * the cosine of its direction. Returns the oracle's error bits. */
+int ora_probe_moller(const gegs_physics *P, int medium, float ekin, uint32_t n, uint64_t seed, float *frac_out,
+                     float *cos_out)
+{
+    ora_region reg[VAC_AND_OTH + 1];
+    memset(reg, 0, sizeof reg);
+    reg[VAC_AND_OTH].med = (uint16_t)medium;
+    reg[VAC_AND_OTH].rhof = 1.0f;
+    ora_stack stk = {0, 0, 0};
+    int64_t tally[1] = {0};
+    ora_ctx C;
+    probe_ctx(&C, &stk, reg, tally, P, NULL, seed);
+    for (uint32_t i = 0; i < n; i++) {
+        ora_particle p;
+        memset(&p, 0, sizeof p);
+        p.e = ekin + P->prm;
+        p.charge = -1;
+        p.wt = 1.0f;
+        p.region = VAC_AND_OTH;
+        p.w = 1.0f;
+        p.status = e_moller;
+        p.rng.hist_lo = i;
+        stk.n = 0;
+        ora_moller(&C, &p);
+        frac_out[i] = -1.0f;
+        cos_out[i] = 2.0f;
+        float emin = 3.0e38f;
+        for (size_t k = 0; k < stk.n; k++)
+            if (stk.a[k].charge == -1 && stk.a[k].e < emin) {
+                emin = stk.a[k].e;
+                frac_out[i] = (stk.a[k].e - P->prm) / ekin;
+                cos_out[i] = stk.a[k].w;
+            }
     }
     free(stk.a);
     return C.error;

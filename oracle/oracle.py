@@ -102,6 +102,17 @@ def probe_compton(physics, medium, flags, energy, n, seed=1):
     return e, c, err
 
 
+def probe_moller(physics, medium, ekin, n, seed=1):
+    """Slower electron's kinetic-energy fraction and direction cosine of n Moller events at `ekin` (MeV)."""
+    L = lib()
+    blk = np.ascontiguousarray(physics)
+    f = np.zeros(n, np.float32)
+    c = np.zeros(n, np.float32)
+    L.ora_probe_moller.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p]
+    err = L.ora_probe_moller(blk.ctypes.data, medium, ekin, n, seed, f.ctypes.data, c.ctypes.data)
+    return f, c, err
+
+
 def probe_rotate(n, seed=1):
     L = lib()
     a = np.zeros(n, np.float32)

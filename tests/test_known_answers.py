@@ -5,6 +5,8 @@ reference's missing test data:
 * the Compton sampler without binding follows the Klein-Nishina cross
   section (chi-square over the scattering cosine) and the Compton relation
   between energy and angle;
+* the Moller sampler follows the Moller cross section above the delta-ray
+  threshold and the two-body relation between energy and angle;
 * direction rotations keep unit length and the requested polar angle;
 * the voxel walk of howfar_phantom visits the voxels an exact ray traversal
   visits, with step lengths adding up to the chord;
@@ -150,3 +152,42 @@ def test_range_table_is_the_integral_of_the_inverse_stopping_power(qel):
         checked += 1
     assert checked >= 10
     assert (np.diff(rng[:L.MXEKE - 1]) > 0).all()      # a range grows with energy
+
+
+def _moller_bin_probs(t, eps_min, edges):
+    """Moller cross section over the slower electron's fraction eps of the kinetic
+    energy, tau = T / mc^2: (1/eps^2)[1 + g2 eps^2 + r^2 - g3 r], r = eps / (1 - eps),
+    g2 = tau^2/(tau+1)^2, g3 = (2 tau + 1)/(tau+1)^2; probability per bin."""
+    tau = t / RM
+    g2 = tau * tau / (tau + 1) ** 2
+    g3 = (2 * tau + 1) / (tau + 1) ** 2
+    e = np.linspace(eps_min, 0.5, 400001)
+    r = e / (1 - e)
+    f = (1 + g2 * e * e + r * (r - g3)) / (e * e)
+    cdf = np.concatenate([[0.0], np.cumsum((f[1:] + f[:-1]) / 2 * np.diff(e))])
+    p = np.diff(np.interp(edges, e, cdf))
+    return p / p.sum()
+
+
+@pytest.mark.parametrize("ekin", [0.6, 2.0, 8.0])
+def test_moller_sampler_follows_the_moller_cross_section(oracle, ekin):
+    """The Moller sampler (without impact ionisation) against the Moller cross
+    section above the delta-ray threshold (chi-square over the energy fraction
+    of the slower electron), and the two-body relation between its energy and
+    its angle."""
+    phys = PD.build_block(["H2O700ICRU"], overrides={"eii_flag": 0})
+    te = float(phys["te"][0])
+    n = 200_000
+    frac, cos, err = oracle.probe_moller(phys, 0, ekin, n, seed=11)
+    assert err == 0 and (frac > 0).all()
+    eps_min = te / ekin
+    assert frac.min() >= eps_min * (1 - 1e-5) and frac.max() <= 0.5 + 1e-6
+    edges = np.linspace(eps_min, 0.5, 41)
+    obs, _ = np.histogram(frac, bins=edges)
+    exp = _moller_bin_probs(ekin, eps_min, edges) * n
+    chi2 = float(((obs - exp) ** 2 / exp).sum())
+    assert chi2 < 40 + 4 * np.sqrt(2 * 40), chi2
+    # cos^2 = (T + 2 mc^2) / T * T2 / (T2 + 2 mc^2) for the electron of kinetic energy T2
+    t2 = frac.astype(np.float64) * ekin
+    want = (ekin + 2 * RM) / ekin * t2 / (t2 + 2 * RM)
+    np.testing.assert_allclose(cos.astype(np.float64) ** 2, want, rtol=2e-4, atol=2e-6)
