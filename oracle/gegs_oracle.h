@@ -35,6 +35,8 @@ int ora_run(const gegs_physics *P, const gegs_scene *S, uint64_t h0, uint64_t h1
 /* Known-answer probes (ora_probe.c). */
 int ora_probe_compton(const gegs_physics *P, int medium, uint32_t flags, float energy, uint32_t n, uint64_t seed,
                       float *e_out, float *cos_out);
+int ora_probe_photo(const gegs_physics *P, int medium, uint32_t flags, float energy, uint32_t n, uint64_t seed,
+                    float *ekin_out, float *cos_out);
 int ora_probe_moller(const gegs_physics *P, int medium, float ekin, uint32_t n, uint64_t seed, float *frac_out,
                      float *cos_out);
 void ora_probe_rotate(uint32_t n, uint64_t seed, float *norm_err, float *cos_err);

@@ -1,6 +1,7 @@
 /* Probes of single oracle routines on controlled inputs, for the project's
  * known-answer tests: the Compton sampler against the analytic Klein-Nishina
- * cross section, the Moller sampler against the Moller cross section,
+ * cross section, the photoelectron direction against the Sauter
+ * distribution, the Moller sampler against the Moller cross section,
  * direction rotations against orthonormality, and the voxel walk of
  * howfar_phantom against an analytic ray traversal.
  * Test infrastructure only (see ora_internal.h). */
@@ -55,6 +56,41 @@ int ora_probe_compton(const gegs_physics *P, int medium, uint32_t flags, float e
         cos_out[i] = 2.0f;
         for (size_t k = 0; k < stk.n; k++)
             if (stk.a[k].charge == 0) { e_out[i] = stk.a[k].e; cos_out[i] = stk.a[k].w; }
+    }
+    free(stk.a);
+    return C.error;
+}
+
+/* n photoelectric events of photons of `energy` along +z in one region of
+ * `medium` with region `flags` (cuts at 0): per event the photoelectron's
+ * kinetic energy and direction cosine (2 when no electron left the event). */
+int ora_probe_photo(const gegs_physics *P, int medium, uint32_t flags, float energy, uint32_t n, uint64_t seed,
+                    float *ekin_out, float *cos_out)
+{
+    ora_region reg[VAC_AND_OTH + 1];
+    memset(reg, 0, sizeof reg);
+    reg[VAC_AND_OTH].med = (uint16_t)medium;
+    reg[VAC_AND_OTH].flags = (uint16_t)flags;
+    reg[VAC_AND_OTH].rhof = 1.0f;
+    ora_stack stk = {0, 0, 0};
+    int64_t tally[1] = {0};
+    ora_ctx C;
+    probe_ctx(&C, &stk, reg, tally, P, NULL, seed);
+    for (uint32_t i = 0; i < n; i++) {
+        ora_particle p;
+        memset(&p, 0, sizeof p);
+        p.e = energy;
+        p.wt = 1.0f;
+        p.region = VAC_AND_OTH;
+        p.w = 1.0f;
+        p.status = p_photo;
+        p.rng.hist_lo = i;
+        stk.n = 0;
+        ora_photo(&C, &p);
+        ekin_out[i] = 0.0f;
+        cos_out[i] = 2.0f;
+        for (size_t k = 0; k < stk.n; k++)
+            if (stk.a[k].charge == -1) { ekin_out[i] = stk.a[k].e - P->prm; cos_out[i] = stk.a[k].w; }
     }
     free(stk.a);
     return C.error;

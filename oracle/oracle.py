@@ -102,6 +102,18 @@ def probe_compton(physics, medium, flags, energy, n, seed=1):
     return e, c, err
 
 
+def probe_photo(physics, medium, flags, energy, n, seed=1):
+    """Photoelectron kinetic energy and direction cosine of n photoelectric events at `energy` (MeV)."""
+    L = lib()
+    blk = np.ascontiguousarray(physics)
+    e = np.zeros(n, np.float32)
+    c = np.zeros(n, np.float32)
+    L.ora_probe_photo.argtypes = [C.c_void_p, C.c_int, C.c_uint32, C.c_float, C.c_uint32, C.c_uint64,
+                                  C.c_void_p, C.c_void_p]
+    err = L.ora_probe_photo(blk.ctypes.data, medium, flags, energy, n, seed, e.ctypes.data, c.ctypes.data)
+    return e, c, err
+
+
 def probe_moller(physics, medium, ekin, n, seed=1):
     """Slower electron's kinetic-energy fraction and direction cosine of n Moller events at `ekin` (MeV)."""
     L = lib()

@@ -5,6 +5,7 @@ reference's missing test data:
 * the Compton sampler without binding follows the Klein-Nishina cross
   section (chi-square over the scattering cosine) and the Compton relation
   between energy and angle;
+* the photoelectron leaves along Sauter's angular distribution;
 * the Moller sampler follows the Moller cross section above the delta-ray
   threshold and the two-body relation between energy and angle;
 * direction rotations keep unit length and the requested polar angle;
@@ -191,3 +192,34 @@ def test_moller_sampler_follows_the_moller_cross_section(oracle, ekin):
     t2 = frac.astype(np.float64) * ekin
     want = (ekin + 2 * RM) / ekin * t2 / (t2 + 2 * RM)
     np.testing.assert_allclose(cos.astype(np.float64) ** 2, want, rtol=2e-4, atol=2e-6)
+
+
+def _sauter_bin_probs(ekin, edges):
+    """Sauter's K-shell photoelectron angular distribution over cos(theta):
+    sin^2 / (1 - beta c)^4 * [1 + gamma (gamma - 1)(gamma - 2) (1 - beta c) / 2]."""
+    g = 1.0 + ekin / RM
+    b = np.sqrt(1.0 - 1.0 / (g * g))
+    c = np.linspace(-1.0, 1.0, 400001)
+    f = (1 - c * c) / (1 - b * c) ** 4 * (1 + 0.5 * g * (g - 1) * (g - 2) * (1 - b * c))
+    cdf = np.concatenate([[0.0], np.cumsum((f[1:] + f[:-1]) / 2 * np.diff(c))])
+    p = np.diff(np.interp(edges, c, cdf))
+    return p / p.sum()
+
+
+@pytest.mark.parametrize("energy", [0.03, 0.1, 0.5])
+def test_photoelectron_direction_follows_sauter(oracle, energy):
+    """With photoelectron angular sampling on and atomic relaxation off, the
+    photoelectron takes the photon's energy and leaves along Sauter's
+    distribution (chi-square over the cosine)."""
+    phys = PD.build_block(["H2O700ICRU"])
+    n = 200_000
+    ekin, cos, err = oracle.probe_photo(phys, 0, 0x20, energy, n, seed=13)
+    assert err == 0 and (cos <= 1.0).all()
+    np.testing.assert_allclose(ekin, energy, rtol=1e-5)
+    edges = np.linspace(-1.0, 1.0, 41)
+    obs, _ = np.histogram(cos, bins=edges)
+    exp = _sauter_bin_probs(energy, edges) * n
+    keep = exp > 5
+    chi2 = float(((obs[keep] - exp[keep]) ** 2 / exp[keep]).sum())
+    dof = int(keep.sum())
+    assert chi2 < dof + 4 * np.sqrt(2 * dof), (chi2, dof)
