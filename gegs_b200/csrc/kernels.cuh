@@ -249,7 +249,9 @@ __device__ __forceinline__ bool refill(const DevCtx &C, int hq, uint32_t n_cont,
 // those steps again, whole, and carries its particles on while their steps
 // need howfar, so that its warps search boundaries with most lanes at once. A
 // step that does not goes back, as it stood, to the first pass of the next
-// wave.
+// wave. For jaws photons the second form (NEAR) is the long-track kernel:
+// it takes the photons still going when the photon phase ended and steps them
+// beside the electron phase.
 template <bool ELEC, int G, bool NEAR = false>
 __device__ __forceinline__ void transport_consumer(const DevCtx &C)
 {
