@@ -1,0 +1,34 @@
+"""The bench's reference arm (the CPU restatement on the host cores) keeps the
+JSON-line contract, and ranks other than 0 print nothing."""
+import json
+import os
+import pathlib
+import subprocess
+import sys
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+ARGS = ["--impl", "reference", "--steps", "1", "--warmup", "1", "--ref-seconds", "0.3", "--nphsp", "20000"]
+
+
+def _run(env_extra=None):
+    env = dict(os.environ, **(env_extra or {}))
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), *ARGS], cwd=ROOT, env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return r.stdout.strip()
+
+
+def test_reference_arm_prints_one_contract_line():
+    out = _run()
+    line = json.loads(out.splitlines()[-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0 and line["higher_is_better"] is True
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["e2e"]["value"] == line["value"]
+
+
+def test_reference_arm_other_ranks_print_nothing():
+    assert _run({"RANK": "1"}) == ""
