@@ -65,12 +65,14 @@ def timeline_summary(eng, args, dims):
     names = eng.TIMELINE_KERNELS
     groups = {"source": [0], "photon transport": [1, 2, 3], "photon interactions": [4, 5, 6, 7],
               "electron transport": [8, 9, 10, 15], "long jaws-photon tracks": [16], "electron interactions": [11, 12, 13, 14]}
-    with np.errstate(all="ignore"):
+    import warnings
+    with np.errstate(all="ignore"), warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)          # waves in which a group did not run
         span = lambda g: np.nan_to_num(np.nanmax(e[:, g], axis=1) - np.nanmin(s[:, g], axis=1))
         phases = {k: float(span(g).sum()) for k, g in groups.items()}
         dur = np.nan_to_num(e - s)
     kern = {names[k]: float(dur[:, k].sum()) for k in range(len(names))}
-    # waves whose photon phase is a photon-jaws launch well past the other kernels of the run
+    # waves whose photon-jaws launch lasts well past every other kernel of the same wave
     pj = dur[:, 1]
     others = np.max(np.delete(dur, [1], axis=1), axis=1)
     lone = (pj > 0.5) & (pj > 2 * others)

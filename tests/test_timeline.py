@@ -34,3 +34,39 @@ def test_wave_timeline_stamps_every_kernel_and_keeps_the_tally(engine):
         assert (first[w[1:]] >= last[w[:-1]]).all()
     finally:
         engine.set_timeline(0)
+
+
+class _FakeEngine:
+    """Two waves of known stamps (ns): wave 1 runs the source, the photon jaws and
+    phantom kernels and the electron phantom kernel; wave 2 only a 2 ms photon-jaws
+    launch. The planner counts waves from 1, so index 0 stays empty."""
+    TIMELINE_KERNELS = ["source", "photon_jaws", "photon_mlc", "photon", "compton", "photo", "rayleigh", "pair",
+                        "electron_jaws", "electron_mlc", "electron", "moller", "brems", "bhabha", "annih",
+                        "electron_near", "photon_jaws_long"]
+
+    def run(self, h0, h1, batch=0):
+        return {"waves": 3, "device_ms": 9.0}
+
+    def set_timeline(self, n):
+        pass
+
+    def timeline(self):
+        tl = np.zeros((8, 32, 2), np.uint64)
+        tl[:, :, 0] = np.iinfo(np.uint64).max
+        ms = 1_000_000
+        for k, (a, b) in {0: (0, 1), 1: (1, 3), 3: (1, 4), 10: (5, 7)}.items():
+            tl[1, k] = (a * ms, b * ms)
+        tl[2, 1] = (8 * ms, 10 * ms)
+        return tl
+
+
+def test_timeline_summary_sums_phases_and_kernels():
+    import types
+    from gegs_b200.profile_case import timeline_summary
+    args = types.SimpleNamespace(first=0, histories=10, batch=0)
+    d = timeline_summary(_FakeEngine(), args, (4, 4, 4))
+    assert d["phase_ms"]["source"] == 1.0
+    assert d["phase_ms"]["photon transport"] == 5.0           # wave 1: 1..4 ms, wave 2: 8..10 ms
+    assert d["phase_ms"]["electron transport"] == 2.0
+    assert d["kernel_ms"]["photon_jaws"] == 4.0 and d["kernel_ms"]["photon"] == 3.0
+    assert d["lone_photon_jaws_waves"] == 1 and d["lone_photon_jaws_ms"] == 2.0
