@@ -70,6 +70,7 @@ struct gegs_engine {
     EStatePk *d_estate[GX_NESTATE] = {};
     uint32_t qcap[GX_NQ] = {};
     uint32_t batch = 0;
+    uint32_t queue_cap = 0;            // gegs_run_opts::queue_cap of the current queues
 
     DevCtx ctx{};
     bool have_physics = false, have_scene = false;
@@ -205,9 +206,40 @@ void gegs_destroy(gegs_engine *e)
     delete e;
 }
 
+gegs_status gegs_check_physics(const gegs_physics *P, char *msg, size_t msg_len)
+{
+    auto fail = [&](const char *text) {
+        if (msg && msg_len) snprintf(msg, msg_len, "%s", text);
+        return GEGS_ERR_ARG;
+    };
+    if (!P) return fail("physics block is NULL");
+    if (P->nmed < 1 || P->nmed > GEGS_MXMED) return fail("physics block: nmed outside 1..GEGS_MXMED");
+    char buf[160];
+#define GX_CHECK_FINITE(name)                                                                        \
+    {                                                                                                \
+        const float *v = (const float *)((const char *)P + offsetof(gegs_physics, name));            \
+        const size_t n = sizeof(((const gegs_physics *)nullptr)->name) / sizeof(float);              \
+        for (size_t i = 0; i < n; i++)                                                               \
+            if (!std::isfinite(v[i])) {                                                              \
+                snprintf(buf, sizeof buf, "physics block: %s[%zu] is not finite", #name, i);         \
+                return fail(buf);                                                                    \
+            }                                                                                        \
+    }
+    GEGS_PHYSICS_FLOAT_MEMBERS(GX_CHECK_FINITE)
+#undef GX_CHECK_FINITE
+    for (int m = 0; m < P->nmed; m++)
+        if (!(P->rho[m] > 0.0f)) return fail("physics block: a medium has a density that is not positive");
+    if (msg && msg_len) msg[0] = '\0';
+    return GEGS_OK;
+}
+
 gegs_status gegs_set_physics(gegs_engine *e, const gegs_physics *P)
 {
     if (!e || !P) return GEGS_ERR_ARG;
+    {
+        char msg[192];
+        if (gegs_check_physics(P, msg, sizeof msg) != GEGS_OK) { e->err = msg; return GEGS_ERR_ARG; }
+    }
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     if (!e->d_P) CK(cudaMalloc(&e->d_P, sizeof(gegs_physics)), "physics");
     CK(cudaMemcpyAsync(e->d_P, P, sizeof(gegs_physics), cudaMemcpyHostToDevice, e->stream), "physics H2D");
@@ -374,18 +406,22 @@ static uint32_t default_batch(gegs_engine *e, uint64_t histories)
     return (uint32_t)want;
 }
 
-static gegs_status ensure_queues(gegs_engine *e, uint32_t batch)
+// Queue buffers for `batch` particles in flight; queue_cap > 0 caps every
+// queue's capacity (a testing aid that makes a run overflow on purpose).
+static gegs_status ensure_queues(gegs_engine *e, uint32_t batch, uint32_t queue_cap)
 {
-    if (batch == e->batch) return GEGS_OK;
+    if (batch == e->batch && queue_cap == e->queue_cap) return GEGS_OK;
     for (int q = 0; q < GX_NQ; q++) {
         uint64_t cap = (uint64_t)(kCapFactor[q] * (float)batch) + 4096;
         if (cap > 0xFFFFFFF0ull) cap = 0xFFFFFFF0ull;
+        if (queue_cap && cap > queue_cap) cap = queue_cap;
         CK(realloc_dev(&e->d_qbuf[q], (size_t)cap), "queue buffer");
         e->qcap[q] = (uint32_t)cap;
     }
     for (int k = 0; k < GX_NESTATE; k++)
         CK(realloc_dev(&e->d_estate[k], (size_t)e->qcap[GX_Q_ECONT + k]), "electron state");
     e->batch = batch;
+    e->queue_cap = queue_cap;
     e->ctx_gen++;
     return GEGS_OK;
 }
@@ -510,7 +546,7 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
         e->ctx.electron_budget = eb;
         e->ctx_gen++;
     }
-    gegs_status st = ensure_queues(e, batch);
+    gegs_status st = ensure_queues(e, batch, o.queue_cap);
     if (st != GEGS_OK) return st;
     fill_queue_ctx(e);
 
@@ -648,6 +684,33 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
     return run_finish(e);
 }
 
+// Fill the engine's run statistics from the device counters of a finished run
+// (stats slots: processed per stage, photon and electron steps, then the steps
+// in the jaws and the MLC per type) and turn the error bits into a status.
+// Stage times and launch counts are left as the run set them.
+static gegs_status finish_stats(gegs_engine *e, uint32_t errbits, const unsigned long long stats[16], uint32_t waves,
+                                float ms)
+{
+    gegs_run_stats &R = e->last;
+    for (int q = 0; q < GX_NSTAGE; q++) R.processed[q] = stats[q];
+    R.photon_steps = stats[GX_NSTAGE];
+    R.electron_steps = stats[GX_NSTAGE + 1];
+    R.photon_steps_class[0] = stats[GX_NSTAGE + 2];
+    R.photon_steps_class[1] = stats[GX_NSTAGE + 3];
+    R.photon_steps_class[2] = R.photon_steps - stats[GX_NSTAGE + 2] - stats[GX_NSTAGE + 3];
+    R.electron_steps_class[0] = stats[GX_NSTAGE + 4];
+    R.electron_steps_class[1] = stats[GX_NSTAGE + 5];
+    R.electron_steps_class[2] = R.electron_steps - stats[GX_NSTAGE + 4] - stats[GX_NSTAGE + 5];
+    R.waves = waves;
+    R.error_bits = errbits;
+    R.device_ms = ms;
+    if (errbits & GX_ERR_QUEUE_FULL) { e->err = "event queue overflow"; return GEGS_ERR_QUEUE_FULL; }
+    if (errbits & GX_ERR_MODULE) { e->err = "particle in an unsupported module"; return GEGS_ERR_MODULE; }
+    if (errbits & GX_ERR_SOURCE) { e->err = "history outside every field range"; return GEGS_ERR_SOURCE; }
+    if (errbits & GX_ERR_STEP_BUDGET) { e->err = "wave budget exhausted"; return GEGS_ERR_STEP_BUDGET; }
+    return GEGS_OK;
+}
+
 static gegs_status run_finish(gegs_engine *e)
 {
     e->in_flight = false;
@@ -660,24 +723,7 @@ static gegs_status run_finish(gegs_engine *e)
     CK(cudaMemcpy(&errbits, e->d_err, sizeof errbits, cudaMemcpyDeviceToHost), "err D2H");
     CK(cudaMemcpy(stats, e->d_stats, sizeof stats, cudaMemcpyDeviceToHost), "stats D2H");
     CK(cudaMemcpy(&hsr, e->d_sched, sizeof hsr, cudaMemcpyDeviceToHost), "sched D2H");
-    gegs_run_stats &R = e->last;
-    for (int q = 0; q < GX_NSTAGE; q++) R.processed[q] = stats[q];
-    R.photon_steps = stats[GX_NSTAGE];
-    R.electron_steps = stats[GX_NSTAGE + 1];
-    R.photon_steps_class[0] = stats[GX_NSTAGE + 2];
-    R.photon_steps_class[1] = stats[GX_NSTAGE + 3];
-    R.photon_steps_class[2] = R.photon_steps - stats[GX_NSTAGE + 2] - stats[GX_NSTAGE + 3];
-    R.electron_steps_class[0] = stats[GX_NSTAGE + 4];
-    R.electron_steps_class[1] = stats[GX_NSTAGE + 5];
-    R.electron_steps_class[2] = R.electron_steps - stats[GX_NSTAGE + 4] - stats[GX_NSTAGE + 5];
-    R.waves = hsr.waves;
-    R.error_bits = errbits;
-    R.device_ms = ms;
-    if (errbits & GX_ERR_QUEUE_FULL) { e->err = "event queue overflow"; return GEGS_ERR_QUEUE_FULL; }
-    if (errbits & GX_ERR_MODULE) { e->err = "particle in an unsupported module"; return GEGS_ERR_MODULE; }
-    if (errbits & GX_ERR_SOURCE) { e->err = "history outside every field range"; return GEGS_ERR_SOURCE; }
-    if (errbits & GX_ERR_STEP_BUDGET) { e->err = "wave budget exhausted"; return GEGS_ERR_STEP_BUDGET; }
-    return GEGS_OK;
+    return finish_stats(e, errbits, stats, hsr.waves, ms);
 }
 
 extern "C" gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts)
@@ -853,6 +899,8 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
 {
     if (!e) return GEGS_ERR_ARG;
     if (!e->have_scene || hist_end < hist_begin) { e->err = "gegs_run_noalloc: no scene, or hist_end < hist_begin"; return GEGS_ERR_ARG; }
+    // a launched run still queued on the engine's stream owns the events and the run statistics
+    if (e->in_flight) { e->err = "a launched run has not been waited for (gegs_wait)"; return GEGS_ERR_ARG; }
     if (batch == 0) batch = GEGS_NOALLOC_MAX_BATCH;
     if (batch > GEGS_NOALLOC_MAX_BATCH) {
         char buf[160];
@@ -906,6 +954,7 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
     hs.batch = batch;
     hs.max_waves = 200000u;
     hs.refill_below = batch / 50u > 0u ? batch / 50u : 1u;
+    hs.pending = 1u;                // k_plan_gated plans only while the run is pending
     cudaStream_t s = e->stream;
     CK(cudaMemsetAsync(base, 0, zero_bytes, s), "gegs_run_noalloc: scratch reset");
     CK(cudaMemcpyAsync(sched, &hs, sizeof hs, cudaMemcpyHostToDevice, s), "gegs_run_noalloc: scheduler H2D");
@@ -914,9 +963,11 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
     CK(cudaEventRecord(e->ev0, s), "event");
     SchedState hsr = {};
     for (uint32_t w = 0; w < hs.max_waves;) {
-        // a few waves between host checks; waves after the last one find empty queues
+        // a few waves between host checks; once a plan has ended the run, the
+        // gated planner injects nothing and counts no wave, and the kernels of
+        // the remaining waves find empty queues
         for (int k = 0; k < 8 && w < hs.max_waves; k++, w++) {
-            k_plan<<<1, 1, 0, s>>>(c, sched);
+            k_plan_gated<<<1, 1, 0, s>>>(c, sched);
             k_source<<<grid, threads, 0, s>>>(c, sched);
             k_photon_jaws<<<grid, threads, 0, s>>>(c);
             k_photon_mlc<<<grid, threads, 0, s>>>(c);
@@ -948,18 +999,9 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
     CK(cudaStreamSynchronize(s), "gegs_run_noalloc: sync");
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e->ev0, e->ev1);
-    gegs_run_stats &R = e->last;
-    R = gegs_run_stats{};
-    for (int q = 0; q < GX_NSTAGE; q++) R.processed[q] = st[q];
-    R.photon_steps = st[GX_NSTAGE];
-    R.electron_steps = st[GX_NSTAGE + 1];
-    R.waves = hsr.waves;
-    R.error_bits = errbits;
-    R.device_ms = ms;
-    if (errbits & GX_ERR_QUEUE_FULL) { e->err = "event queue overflow"; return GEGS_ERR_QUEUE_FULL; }
-    if (errbits & GX_ERR_MODULE) { e->err = "particle in an unsupported module"; return GEGS_ERR_MODULE; }
-    if (errbits & GX_ERR_SOURCE) { e->err = "history outside every field range"; return GEGS_ERR_SOURCE; }
-    if (errbits & GX_ERR_STEP_BUDGET) { e->err = "wave budget exhausted"; return GEGS_ERR_STEP_BUDGET; }
+    e->last = gegs_run_stats{};
+    gegs_status fs = finish_stats(e, errbits, st, hsr.waves, ms);
+    if (fs != GEGS_OK) return fs;
     if (hsr.pending) { e->err = "wave budget exhausted"; return GEGS_ERR_STEP_BUDGET; }
     return GEGS_OK;
 }

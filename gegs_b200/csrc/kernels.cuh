@@ -502,6 +502,19 @@ __global__ void k_plan(const __grid_constant__ DevCtx C, SchedState *st)
     plan_wave(C, st);
 }
 
+// Planner of a host-driven loop that queues several waves between checks
+// (gegs_run_noalloc): once a plan has ended the run (pending 0), later calls
+// inject nothing and count no wave, so the run's wave count and injected
+// histories are those of the graph form, which stops at that plan.
+__global__ void k_plan_gated(const __grid_constant__ DevCtx C, SchedState *st)
+{
+    if (st->pending == 0u) {
+        st->h0 = st->h1 = st->next;
+        return;
+    }
+    plan_wave(C, st);
+}
+
 __global__ void k_plan_cond(const __grid_constant__ DevCtx C, SchedState *st, cudaGraphConditionalHandle handle)
 {
     uint32_t pending = plan_wave(C, st);

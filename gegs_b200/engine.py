@@ -20,7 +20,8 @@ MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 
 EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_set_timeline", "gegs_get_timeline", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
            "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_set_tally", "gegs_get_dose", "gegs_get_stats",
-           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version"]
+           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version",
+           "gegs_check_physics"]
 
 
 TRACE_DTYPE = np.dtype([("kind_stage", "<u4"), ("hist_lo", "<u4"), ("sid_lo", "<u4"), ("sid_hi", "<u4"),
@@ -36,7 +37,7 @@ class GegsError(RuntimeError):
 class RunOpts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("batch", C.c_uint32), ("blocks_per_sm", C.c_int32),
                 ("threads_per_block", C.c_int32), ("max_waves", C.c_uint32), ("step_budget", C.c_uint32),
-                ("refill_below", C.c_uint32)]
+                ("refill_below", C.c_uint32), ("queue_cap", C.c_uint32)]
 
 
 class RunStats(C.Structure):
@@ -83,9 +84,21 @@ def load_library(path=None):
     for f in ("gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field"):
         getattr(L, f).restype = C.c_size_t
     L.gegs_version.restype = C.c_char_p
+    L.gegs_check_physics.argtypes = [vp, C.c_char_p, C.c_size_t]
     if path is None:
         _lib = L
     return L
+
+
+def check_physics(block: np.ndarray):
+    """Host-side validation of a physics block through the C ABI (no GPU
+    needed); raises GegsError naming the first bad entry."""
+    L = load_library()
+    blk = np.ascontiguousarray(block)
+    msg = C.create_string_buffer(192)
+    st = L.gegs_check_physics(blk.ctypes.data, msg, len(msg))
+    if st != 0:
+        raise GegsError(st, msg.value.decode())
 
 
 class Engine:
@@ -140,7 +153,7 @@ class Engine:
         if g.size != self.nvox:
             raise ValueError(f"voxel gradient has {g.size} entries for {self.nvox} voxels")
         out = np.zeros(self.nbeamlets, np.float64)
-        o = RunOpts(MODE_PERSISTENT, batch, 0, 0, 0, 0, 0)
+        o = RunOpts(MODE_PERSISTENT, batch, 0, 0, 0, 0, 0, 0)
         self._check(self.L.gegs_backward(self.h, h0, h1, g.ctypes.data, out.ctypes.data, out.size, C.byref(o)))
         return out
 
@@ -150,9 +163,9 @@ class Engine:
 
     def run(self, h0: int, h1: int, mode: int = MODE_PERSISTENT, batch: int = 0, blocks_per_sm: int = 0,
             threads: int = 0, max_waves: int = 0, photon_budget: int = 0, electron_budget: int = 0,
-            refill_below: int = 0):
+            refill_below: int = 0, queue_cap: int = 0):
         o = RunOpts(mode, batch, blocks_per_sm, threads, max_waves, (photon_budget & 0xFFFF) | (electron_budget << 16),
-                    refill_below)
+                    refill_below, queue_cap)
         self._check(self.L.gegs_run(self.h, h0, h1, C.byref(o)))
         return self.stats()
 
@@ -160,7 +173,7 @@ class Engine:
                photon_budget: int = 0, electron_budget: int = 0, refill_below: int = 0):
         """Queue a persistent-form run and return at once (see wait())."""
         o = RunOpts(MODE_PERSISTENT, batch, blocks_per_sm, threads, 0, (photon_budget & 0xFFFF) | (electron_budget << 16),
-                    refill_below)
+                    refill_below, 0)
         self._check(self.L.gegs_launch(self.h, h0, h1, C.byref(o)))
 
     def wait(self):

@@ -120,7 +120,14 @@ def read_egsphant(path):
             raise ValueError(f"{path}: medium name {i} is empty")
         media.append(name)
     k += 1                                   # ESTEPE line
-    nx, ny, nz = (int(t) for t in lines[k].split()[:3]); k += 1
+    try:
+        nx, ny, nz = (int(t) for t in lines[k].split()[:3])
+    except (ValueError, IndexError):
+        raise ValueError(f"{path}: line {k + 1} must hold the three voxel counts nx ny nz, "
+                         f"got {lines[k] if k < len(lines) else ''!r}") from None
+    if min(nx, ny, nz) < 1:
+        raise ValueError(f"{path}: voxel counts {nx} {ny} {nz} must be positive")
+    k += 1
     rest = StreamReader("\n".join(lines[k:]))
     xb = np.array([rest.num() for _ in range(nx + 1)], np.float32)
     yb = np.array([rest.num() for _ in range(ny + 1)], np.float32)
@@ -187,10 +194,15 @@ def read_egsphsp1_header(path):
     n, nphot = struct.unpack("<ii", head[5:13])
     ekmax, ekmin = struct.unpack("<ff", head[13:21])
     order = "<"
-    if n < 0 or n > (os.path.getsize(path) // 28):   # written on a big-endian machine
-        order = ">"
-        n, nphot = struct.unpack(">ii", head[5:13])
-        ekmax, ekmin = struct.unpack(">ff", head[13:21])
+    held = os.path.getsize(path) // 28
+    if n < 0 or n > held:                 # written on a big-endian machine, or truncated
+        n_be, nphot_be = struct.unpack(">ii", head[5:13])
+        if 0 <= n_be <= held:
+            order = ">"
+            n, nphot = n_be, nphot_be
+            ekmax, ekmin = struct.unpack(">ff", head[13:21])
+        elif n < 0:
+            raise ValueError(f"{path}: negative particle count {n} in the header")
     return dict(mode=mode, n=n, nphot=nphot, ekmax=ekmax, ekmin=ekmin, order=order,
                 reclen=28 if mode == "MODE0" else 32)
 
@@ -202,6 +214,10 @@ def read_egsphsp1(path, start=0, count=None):
     dt = PHSP_DTYPE if h["mode"] == "MODE0" else _PHSP2_DTYPE
     if h["order"] == ">":
         dt = dt.newbyteorder(">")
+    held = os.path.getsize(path) // h["reclen"] - 1          # records after the header record
+    if h["n"] > held:
+        raise ValueError(f"{path}: the header announces {h['n']} particles but the file holds {max(held, 0)} "
+                         f"records (truncated)")
     with open(path, "rb") as f:
         f.seek(h["reclen"] * (1 + start))
         raw = np.fromfile(f, dtype=dt, count=max(n, 0))

@@ -165,7 +165,14 @@ def render_header() -> str:
         ctype = "float" if kind == F else "int32_t"
         dims = "".join(f"[{d}]" for d in shape)
         out.append(f"    {ctype} {name}{dims};\n")
-    out.append("} gegs_physics;\n\n#endif /* GEGS_PHYSICS_H */\n")
+    out.append("} gegs_physics;\n\n")
+    out.append("/* X-macro over the float members (every value must be finite; checked by\n"
+               " * gegs_check_physics before a block is used). */\n")
+    out.append("#define GEGS_PHYSICS_FLOAT_MEMBERS(X) \\\n")
+    names = [name for name, kind, _ in FIELDS if kind == F]
+    for i, name in enumerate(names):
+        out.append(f"    X({name})" + (" \\\n" if i + 1 < len(names) else "\n"))
+    out.append("\n#endif /* GEGS_PHYSICS_H */\n")
     return "".join(out)
 
 

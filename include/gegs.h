@@ -65,6 +65,10 @@ typedef struct gegs_run_opts {
                                   8x theirs in the jaws and MLC, electrons 2x theirs in the phantom */
     uint32_t refill_below;     /* new histories are injected once fewer than this many particles are in
                                   flight, topping the population up to `batch` (0 = default batch / 4) */
+    uint32_t queue_cap;        /* testing aid: at most this many records per event queue (0 = sized from
+                                  `batch`). A queue that would overflow drops nothing silently: the run
+                                  stops after the wave and returns GEGS_ERR_QUEUE_FULL (the reference
+                                  drops the particle with a message, utility.cu:270-275) */
 } gegs_run_opts;
 
 typedef struct gegs_run_stats {
@@ -88,8 +92,15 @@ void gegs_destroy(gegs_engine *e);
 const char *gegs_last_error(const gegs_engine *e);
 
 /* Physics tables (struct gegs_physics, same layout the reference keeps in
- * __device__ globals); copied to HBM. */
+ * __device__ globals); checked with gegs_check_physics, then copied to HBM. */
 gegs_status gegs_set_physics(gegs_engine *e, const gegs_physics *P);
+
+/* Host-only check of a physics block (no GPU needed): nmed in 1..GEGS_MXMED,
+ * every float member finite, every used medium's density positive. Returns
+ * GEGS_ERR_ARG and a message naming the first bad entry (msg may be NULL).
+ * The reference has no such check: its HATCH readers trust the data files
+ * (media.cu:332-830). */
+gegs_status gegs_check_physics(const gegs_physics *P, char *msg, size_t msg_len);
 
 /* Phantom, beam-line geometry, fields and phase space; all copied to HBM.
  * Resets the tally. */

@@ -162,4 +162,83 @@ typedef struct gegs_physics {
     int32_t eii_no[60];
 } gegs_physics;
 
+/* X-macro over the float members (every value must be finite; checked by
+ * gegs_check_physics before a block is used). */
+#define GEGS_PHYSICS_FLOAT_MEMBERS(X) \
+    X(rm) \
+    X(prm) \
+    X(rmt2) \
+    X(rmsq) \
+    X(estepe) \
+    X(ximax) \
+    X(skindepth_for_bca) \
+    X(rho) \
+    X(ae) \
+    X(ap) \
+    X(ue) \
+    X(up) \
+    X(te) \
+    X(thmoll) \
+    X(rlc) \
+    X(delcm) \
+    X(zbrang) \
+    X(lzbrang) \
+    X(log_ap) \
+    X(blcc) \
+    X(xcc) \
+    X(expeke1) \
+    X(smaxir) \
+    X(e_max_rr) \
+    X(zelem) \
+    X(pz) \
+    X(wa) \
+    X(dl1) \
+    X(dl2) \
+    X(dl3) \
+    X(dl4) \
+    X(dl5) \
+    X(dl6) \
+    X(bpar) \
+    X(ge) \
+    X(gmfp) \
+    X(gbr1) \
+    X(gbr2) \
+    X(cohe) \
+    X(pmax) \
+    X(rayleigh_data) \
+    X(eke01) \
+    X(sig) \
+    X(dedx) \
+    X(ebr1) \
+    X(pbr1) \
+    X(pbr2) \
+    X(tmxs) \
+    X(range_ep) \
+    X(e_array) \
+    X(sig_e) \
+    X(binding_energies) \
+    X(interaction_prob) \
+    X(relaxation_prob) \
+    X(edge_energies) \
+    X(edge_a) \
+    X(edge_b) \
+    X(edge_c) \
+    X(edge_d) \
+    X(be_array) \
+    X(jo_array) \
+    X(erfjo_array) \
+    X(eno_array) \
+    X(llammin) \
+    X(llammax) \
+    X(dllamb) \
+    X(dllambi) \
+    X(dqms) \
+    X(dqmsi) \
+    X(ums_array) \
+    X(fms_array) \
+    X(wms_array) \
+    X(eii_xsection) \
+    X(eii_cons) \
+    X(eii)
+
 #endif /* GEGS_PHYSICS_H */

@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 from gegs_b200 import workloads as W
-from gegs_b200.engine import GegsError
+from gegs_b200.engine import MODE_TIMED, GegsError
 
 pytestmark = pytest.mark.gpu
 
@@ -65,3 +65,44 @@ def test_noalloc_rejects_batch_above_the_fixed_limit(engine):
     assert err.value.status == 1
     assert "GEGS_NOALLOC_MAX_BATCH" in str(err.value)
     _noalloc(engine, 0, 100, batch=MAX_BATCH)    # the limit itself is accepted
+
+
+def test_noalloc_counts_waves_and_steps_like_the_timed_form(engine):
+    # The timed form launches the same kernels wave by wave, one at a time;
+    # with the same batch, refill threshold and step budgets it plans the same
+    # waves, so the statistics (waves, per-stage counts, steps per geometry
+    # class) agree as well as the tally.
+    job = W.config3(histories=3000, nphsp=3000, dims=(40, 40, 20))
+    engine.set_physics(job.physics)
+    engine.set_scene(job.scene())
+    engine.reset_tally()
+    ref = engine.run(0, job.histories, mode=MODE_TIMED, batch=1024, refill_below=1024 // 50,
+                     photon_budget=16, electron_budget=8)
+    ref_tally = engine.tally()
+    engine.reset_tally()
+    _noalloc(engine, 0, job.histories, batch=1024)
+    got = engine.stats()
+    np.testing.assert_array_equal(engine.tally(), ref_tally)
+    for key in ("waves", "processed", "photon_steps", "electron_steps", "photon_steps_class",
+                "electron_steps_class"):
+        assert got[key] == ref[key], key
+
+
+def test_noalloc_refuses_while_a_launched_run_is_outstanding(engine):
+    # gegs_launch leaves a run queued on the engine's stream; the no-allocation
+    # call must not queue behind it and take over its events and statistics.
+    job = W.config1(histories=2000, n=16, voxel=2.0)
+    engine.set_physics(job.physics)
+    engine.set_scene(job.scene())
+    engine.reset_tally()
+    engine.launch(0, job.histories)
+    with pytest.raises(GegsError) as err:
+        _noalloc(engine, 0, job.histories)
+    assert err.value.status == 1
+    assert "gegs_wait" in str(err.value)
+    st = engine.wait()
+    launched = engine.tally()
+    assert st["error_bits"] == 0 and launched.sum() > 0
+    engine.reset_tally()
+    _noalloc(engine, 0, job.histories)            # usable again once the launched run is waited for
+    np.testing.assert_array_equal(engine.tally(), launched)
