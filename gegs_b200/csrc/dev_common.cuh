@@ -58,9 +58,12 @@ static_assert(sizeof(gegs_field) % 16 == 0, "field record size");
 #define GX_NESTATE 8
 #define GX_TL_KERNELS 32   // wave timeline slots per wave
 #define GX_LOOP_CAP 1000
-#define GX_EPSGMFP 1.e-5f
-#define GX_EPSEMFP 1.e-5f
-#define GX_EPSTEP 0.0005f
+// The reference's step constants are double literals (EGSnrc_Parameters.h:91-92,
+// CUDA_EGS.h:34): a step that adds EPSTEP, and a comparison with EPSGMFP or
+// EPSEMFP, is evaluated in double, as there. (INFI_DIST, 1e5, is exact in float.)
+#define GX_EPSGMFP 1.e-5
+#define GX_EPSEMFP 1.e-5
+#define GX_EPSTEP 0.0005
 #define GX_INFI_DIST 1e5f
 #define GX_OUTMLC (-99)
 #define GX_PASSMLC (-98)

@@ -14,7 +14,7 @@ __device__ __forceinline__ float ev2(float2 t, float x) { return t.x + t.y * x; 
 __device__ void mscat(const DevCtx &C, float lambda, float chia2, float q1, float &cost, float &sint, Rng &r)
 {
     const gegs_physics *P = C.P;
-    if (lambda <= 13.8f) {
+    if (lambda <= 13.8) {
         float sprob = U(C, r);
         float explambda = gx_exp(-lambda);
         if (sprob < explambda) { cost = 1.0f; sint = 0.0f; return; }
@@ -41,20 +41,23 @@ __device__ void mscat(const DevCtx &C, float lambda, float chia2, float q1, floa
                 xi = 2.0f * chia2 * xi / (1.0f - xi + chia2);
                 float cosz = 1.0f - xi;
                 float sinz = xi * (2.0f - xi);
-                if (sinz > 1.0e-20f) {
+                if (sinz > 1.0e-20) {
                     sinz = sqrtf(sinz);
                     xi = U(C, r);
-                    float phi = xi * 6.2831853f;
+                    float phi = xi * 6.2831853;
                     float sp, cp;
                     gx_sincos(phi, &sp, &cp);
                     cost = cost * cosz - sint * sinz * cp;
-                    sint = sqrtf(fmaxf_(0.0f, (1.0f - cost) * (1.0f + cost)));
+                    // sqrt(max(0.0, x)) in double (electron.cu:160), rounded to float:
+                    // +0 for x <= 0, else the correctly rounded square root of x
+                    const float sx = (1.0f - cost) * (1.0f + cost);
+                    sint = sx > 0.0f ? sqrtf(sx) : 0.0f;
                 }
             } while (wsum <= sprob);
             return;
         }
     }
-    if (lambda <= 1e5f) {
+    if (lambda <= 1e5) {
         float llmbda = gx_log(lambda);
         float ai = llmbda * P->dllambi;
         int msi = (int)ai;
@@ -63,7 +66,7 @@ __device__ void mscat(const DevCtx &C, float lambda, float chia2, float q1, floa
         if (xi < ai) msi = msi + 1;
         if (msi > GEGS_MAXL_MS) msi = GEGS_MAXL_MS;
         int msj;
-        if (q1 < 1e-3f) msj = 0;
+        if (q1 < 1e-3) msj = 0;
         else if (q1 < 0.5f) {
             float aj = q1 * P->dqmsi;
             msj = (int)aj;
@@ -72,10 +75,10 @@ __device__ void mscat(const DevCtx &C, float lambda, float chia2, float q1, floa
             if (xi < aj) msj = msj + 1;
         } else msj = GEGS_MAXQ_MS;
         float omega2;
-        if (llmbda < 2.2299f)
-            omega2 = chia2 * (lambda + 4.0f) * (1.347006f + llmbda * (0.209364f - llmbda * (0.45525f - llmbda * (0.50142f - 0.081234f * llmbda))));
+        if (llmbda < 2.2299)
+            omega2 = chia2 * (lambda + 4) * (1.347006 + llmbda * (0.209364 - llmbda * (0.45525 - llmbda * (0.50142 - 0.081234 * llmbda))));
         else
-            omega2 = chia2 * (lambda + 4.0f) * (-2.77164f + llmbda * (2.94874f - llmbda * (0.1535754f - llmbda * 0.00552888f)));
+            omega2 = chia2 * (lambda + 4) * (-2.77164 + llmbda * (2.94874 - llmbda * (0.1535754 - llmbda * 0.00552888)));
         xi = U(C, r);
         float ak = xi * (float)GEGS_MAXU_MS;
         int msk = (int)ak;
@@ -91,13 +94,13 @@ __device__ void mscat(const DevCtx &C, float lambda, float chia2, float q1, floa
         float u = __ldg(&P->ums_array[idx]);
         float du = __ldg(&P->ums_array[((msk + 1) * sj + msj) * sl + msi]) - u;
         xi = U(C, r);
-        if (fabsf(a) < 0.2f) {
-            float x1 = 0.5f * (1.0f - xi) * a;
+        if (fabsf(a) < 0.2) {
+            float x1 = 0.5 * (1 - xi) * a;
             u = u + xi * du * (1.0f + x1 * (1.0f - xi * a));
         } else
             u = u - du / a * (1.0f - sqrtf(1.0f + xi * a * (2.0f + a)));
-        xi = omega2 * u / (1.0f + 0.5f * omega2 - u);
-        if (xi > 1.99999f) xi = 1.99999f;
+        xi = omega2 * u / (1 + 0.5 * omega2 - u);
+        if (xi > 1.99999) xi = 1.99999;
         cost = 1.0f - xi;
         sint = sqrtf(xi * (2.0f - xi));
         return;
@@ -121,15 +124,15 @@ __device__ void msdist_pI(const DevCtx &C, float eloss, float tustep, Part &p0, 
     float e0 = p0.e - P->rm;
     float blccc = P->blcc[medium];
     float xcccc = P->xcc[medium];
-    float e = e0 - 0.5f * eloss;
+    float e = e0 - 0.5 * eloss;
     float p2 = e * (e + P->rmt2);
     float chia2 = xcccc / p2 / (4.0f * blccc);
     float beta2 = p2 / (p2 + P->rmsq);
     float lambda = tustep * rd.rhof * blccc / beta2;
-    float factor = 1.0f / (1.0f + 0.9784671f * e);
+    float factor = 1 / (1 + 0.9784671 * e);
     float epsilon = eloss / e0;
-    epsilon = epsilon / (1.0f - 0.5f * epsilon);
-    float temp = 0.25f * (1.0f - factor * (1.0f - 0.333333f * factor)) * epsilon * epsilon;
+    epsilon = epsilon / (1 - 0.5 * epsilon);
+    float temp = 0.25 * (1 - factor * (1 - 0.333333 * factor)) * epsilon * epsilon;
     lambda = lambda * (1.0f + temp);
     lambda = lambda / (1.0f + chia2);
     float chilog = gx_log(1.0f + 1.0f / chia2);
@@ -142,9 +145,9 @@ __device__ void msdist_pI(const DevCtx &C, float eloss, float tustep, Part &p0, 
     float us = sint * cphi;
     float vs = sint * sphi;
     float z, rr, r2, z2, r2max;
-    if (xi < 0.1f) z = 1.0f - xi * (0.5f - xi * (0.166666667f - 0.041666667f * xi));
+    if (xi < 0.1) z = 1 - xi * (0.5 - xi * (0.166666667 - 0.041666667 * xi));
     else z = (1.0f - gx_exp(-xi)) / xi;
-    rr = 0.5f * sint;
+    rr = 0.5 * sint;
     r2 = rr * rr;
     z2 = z * z;
     r2max = 1.0f - z2;
@@ -152,7 +155,7 @@ __device__ void msdist_pI(const DevCtx &C, float eloss, float tustep, Part &p0, 
     float ut = rr * cphi, vt = rr * sphi, wt = z;
     ustep = sqrtf(z2 + r2) * tustep;
     float sint02 = p0.u * p0.u + p0.v * p0.v;
-    if (sint02 > 1e-20f) {
+    if (sint02 > 1e-20) {
         float sint0 = sqrtf(sint02);
         float cphi0 = p0.u / sint0;
         float sphi0 = p0.v / sint0;
@@ -179,7 +182,7 @@ __device__ void msdist_pI(const DevCtx &C, float eloss, float tustep, Part &p0, 
 __device__ __forceinline__ float range_piece(const gegs_physics *P, int qel, unsigned medium, int lel, float elk_a, float elk_b,
                                              float e_hi, float fedep)
 {
-    float elktmp = 0.5f * (elk_a + elk_b + 0.25f * fedep * fedep * (1.0f + fedep * (1.0f + 0.875f * fedep)));
+    float elktmp = 0.5 * (elk_a + elk_b + 0.25 * fedep * fedep * (1 + fedep * (1 + 0.875 * fedep)));
     float2 d = tab2(P->dedx, qel * GX_MXEKE * GX_MXMED + medium * GX_MXEKE + lel - 1);
     float dedxmid = d.x + d.y * elktmp;
     dedxmid = 1.0f / dedxmid;
@@ -201,11 +204,11 @@ __device__ float compute_eloss(const gegs_physics *P, int qel, unsigned medium, 
         float aux = d.y / dedxmid;
         de = dedxmid * step * rhof;
         float fedep = de / eke_val;
-        de = de * (1.0f - 0.5f * fedep * aux * (1.0f - 0.333333f * fedep * (aux - 1.0f - 0.25f * fedep * (2.0f - aux * (4.0f - aux)))));
+        de = de * (1 - 0.5 * fedep * aux * (1 - 0.333333 * fedep * (aux - 1 - 0.25 * fedep * (2 - aux * (4 - aux)))));
     } else {
         int lelktmp = lelke;
         tuss = (range - step) * rhof;
-        if (tuss <= 0.0f) de = eke_val - P->te[medium] * 0.99f;
+        if (tuss <= 0.0f) de = eke_val - P->te[medium] * 0.99;
         else {
             while (lelktmp > 1 && tuss < __ldg(&P->range_ep[(medium * GX_MXEKE + lelktmp - 1) * 2 + qel])) lelktmp = lelktmp - 1;
             float elktmp = ((float)(lelktmp + 1) - ex.x) / ex.y;
@@ -216,7 +219,7 @@ __device__ float compute_eloss(const gegs_physics *P, int qel, unsigned medium, 
             float aux = d.y / dedxmid;
             de = dedxmid * tuss * rhof;
             float fedep = de / eketmp;
-            de = de * (1.0f - 0.5f * fedep * aux * (1.0f - 0.333333f * fedep * (aux - 1.0f - 0.25f * fedep * (2.0f - aux * (4.0f - aux)))));
+            de = de * (1 - 0.5 * fedep * aux * (1 - 0.333333 * fedep * (aux - 1 - 0.25 * fedep * (2 - aux * (4 - aux)))));
             de = de + eke_val - eketmp;
         }
     }
@@ -374,23 +377,23 @@ __device__ int electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
                 float rnnoss = U(C, r);
                 float lambda = -gx_log(1.0f - rnnoss);
                 float tmp = (eke_val / rm + 1.0f);
-                float lambda_max = 0.5f * blccl * rm / dedx_val * tmp * tmp * tmp;
+                float lambda_max = 0.5 * blccl * rm / dedx_val * tmp * tmp * tmp;
                 if (lambda >= 0.0f && lambda_max > 0.0f) {
                     float tuss;
-                    if (lambda < lambda_max) tuss = lambda * ssmfp * (1.0f - 0.5f * lambda / lambda_max);
-                    else tuss = 0.5f * lambda * ssmfp;
+                    if (lambda < lambda_max) tuss = lambda * ssmfp * (1 - 0.5 * lambda / lambda_max);
+                    else tuss = 0.5 * lambda * ssmfp;
                     if (tuss < tustep) { tustep = tuss; dosingle = true; } else dosingle = false;
                 } else return true;
                 ustep = tustep;
             } else {
                 domultiple = true;
-                float ekems = eke_val - 0.5f * tustep * dedx_val;
+                float ekems = eke_val - 0.5 * tustep * dedx_val;
                 p2 = ekems * (ekems + rmt2);
                 beta2 = p2 / (p2 + rmsq);
                 chia2 = xccl / (4.0f * blccl * p2);
-                xi = 0.5f * xccl / p2 / beta2 * tustep;
-                xi = xi * (gx_log(1.0f + 1.0f / chia2) - 1.0f / (1.0f + chia2));
-                if (xi < 0.1f) ustep = tustep * (1.0f - xi * (0.5f - xi * 0.166667f));
+                xi = 0.5 * xccl / p2 / beta2 * tustep;
+                xi = xi * (gx_log((float)(1 + 1.0 / chia2)) - 1 / (1 + chia2));
+                if (xi < 0.1) ustep = tustep * (1 - xi * (0.5 - xi * 0.166667));
                 else ustep = tustep * (1.0f - gx_exp(-xi)) / xi;
             }
             callhowfar = !(ustep < tperp);
@@ -439,15 +442,15 @@ __device__ int electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
             if (tvstep != tustep) dosingle = false;
         } else {
             if (vstep < ustep0) {
-                float ekems = eke_val - 0.5f * tustep * vstep / ustep0 * dedx_val;
+                float ekems = eke_val - 0.5 * tustep * vstep / ustep0 * dedx_val;
                 float p2 = ekems * (ekems + rmt2);
                 beta2 = p2 / (p2 + rmsq);
                 chia2 = xccl / (4.0f * blccl * p2);
-                xi = 0.5f * xccl / p2 / beta2 * vstep;
-                xi = xi * (gx_log(1.0f + 1.0f / chia2) - 1.0f / (1.0f + chia2));
-                if (xi < 0.1f) tvstep = vstep * (1.0f + xi * (0.5f + xi * 0.333333f));
+                xi = 0.5 * xccl / p2 / beta2 * vstep;
+                xi = xi * (gx_log((float)(1 + 1.0 / chia2)) - 1 / (1 + chia2));
+                if (xi < 0.1) tvstep = vstep * (1 + xi * (0.5 + xi * 0.333333));
                 else {
-                    if (xi < 0.999999f) tvstep = -vstep * gx_log(1.0f - xi) / xi;
+                    if (xi < 0.999999) tvstep = -vstep * gx_log(1 - xi) / xi;
                     else return true;
                 }
             } else tvstep = tustep;
@@ -506,7 +509,7 @@ __device__ int electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
     if (medium != medold) { s.is_tstep = true; return false; }
     s.demfp = s.demfp - save_de * sig_val;
     s.total_tstep = s.total_tstep - tvstep * rhof;
-    if (s.total_tstep < 1e-9f) s.demfp = 0.0f;
+    if (s.total_tstep < 1e-9) s.demfp = 0.0f;
     if (s.demfp >= GX_EPSEMFP) { s.is_tstep = false; return false; }
     float sigf = ev2(tab2(P->sig, qel * GX_MXEKE * GX_MXMED + medium * GX_MXEKE + s.lelke - 1), s.elke);
     float dedx0 = ev2(tab2(P->dedx, qel * GX_MXEKE * GX_MXMED + medium * GX_MXEKE + s.lelke - 1), s.elke);
@@ -547,12 +550,12 @@ __device__ void eii_sample(const DevCtx &C, int ish, int iz, float uj, Part &p, 
     float tau12 = (tau + 1.0f) * (tau + 1.0f);
     float p2 = tau * tau + 2.0f * tau;
     float beta2 = p2 / tau12;
-    float wmax = 0.5f * (t + uj);
+    float wmax = 0.5 * (t + uj);
     float xmax = uj / wmax;
     float c1 = (wmax / eie) * (wmax / eie);
     float c2 = (2.0f * tau + 1.0f) / tau12;
     float fm_s = gx_log(rmt2 * p2 / uj) - beta2 - 0.5f;
-    float prob_s = 0.66666667f * fm_s * (1.0f + xmax + xmax * xmax);
+    float prob_s = 0.66666667 * fm_s * (1 + xmax + xmax * xmax);
     float fm_h = 2.0f + c1 - c2;
     if (fm_h < 1.0f) fm_h = 1.0f;
     float prob = fm_h + prob_s;
@@ -620,7 +623,7 @@ __device__ void moller(const DevCtx &C, Part p, Rng &r)
         rsh = sigm * rsh;
         int nne = P->nne[medium];
         for (int iele = 0; iele < nne; iele++) {
-            int iz = (int)(__ldg(&P->zelem[iele * GX_MXMED + medium]) + 0.5f);
+            int iz = (int)(__ldg(&P->zelem[iele * GX_MXMED + medium]) + 0.5);
             int nsh = __ldg(&P->eii_no[iele * GX_MXMED + medium]);
             if (nsh > 0) {
                 int ifirst = __ldg(&P->eii_first[iele * GX_MXMED + medium]);
@@ -656,7 +659,7 @@ __device__ void moller(const DevCtx &C, Part p, Rng &r)
     float e02 = e0 * e0;
     float g2 = t0 * t0 / e02;
     float g3 = (2.0f * t0 + 1.0f) / e02;
-    float gmax = (1.0f + 1.25f * g2);
+    float gmax = (1.0f + 1.25 * g2);
     float rnno27, rejf4, br, rr;
     int n = 0;
     do {
@@ -700,7 +703,7 @@ __device__ void brems(const DevCtx &C, Part p, Rng &r)
     int nbr = P->nbr_split;
     if (nbr < 1) return;
     float eie = p.e;
-    int l = (eie < 50.0f) ? 1 : 3;
+    int l = (eie < 50.0) ? 1 : 3;
     int l1 = l + 1;
     float ekin = eie - prm;
     float elke = gx_log(ekin);
@@ -712,7 +715,7 @@ __device__ void brems(const DevCtx &C, Part p, Rng &r)
     if (ibrdst >= 0) {
         a = p.u; b = p.v; c = p.w;
         sinpsi = a * a + b * b;
-        if (sinpsi > 1e-20f) {
+        if (sinpsi > 1e-20) {
             sinpsi = sqrtf(sinpsi);
             sindel = b / sinpsi;
             cosdel = a / sinpsi;
@@ -788,7 +791,7 @@ __device__ void brems(const DevCtx &C, Part p, Rng &r)
             float sinthe = sqrtf(fmaxf_((1.0f - costhe) * (1.0f + costhe), 0.0f));
             float cphi, sphi;
             box_phi(C, r, cphi, sphi);
-            if (sinpsi >= 1e-10f) {
+            if (sinpsi >= 1e-10) {
                 float us = sinthe * cphi;
                 float vs = sinthe * sphi;
                 p1.u = c * cosdel * us - sindel * vs + a * costhe;
@@ -888,7 +891,7 @@ __device__ void annih(const DevCtx &C, Part p, Rng &r)
     float wsamp = gx_log((1.0f - ep0) / ep0);
     float aa = p.u, bb = p.v, cc = p.w;
     float sinpsi = aa * aa + bb * bb, sindel = 0.0f, cosdel = 0.0f;
-    if (sinpsi > 1e-20f) {
+    if (sinpsi > 1e-20) {
         sinpsi = sqrtf(sinpsi);
         sindel = bb / sinpsi;
         cosdel = aa / sinpsi;
@@ -910,7 +913,7 @@ __device__ void annih(const DevCtx &C, Part p, Rng &r)
         float sinthe = sqrtf(1.0f - costhe * costhe);
         float cphi, sphi;
         box_phi(C, r, cphi, sphi);
-        if (sinpsi >= 1e-10f) {
+        if (sinpsi >= 1e-10) {
             float us = sinthe * cphi, vs = sinthe * sphi;
             p.u = cc * cosdel * us - sindel * vs + aa * costhe;
             p.v = cc * sindel * us + cosdel * vs + bb * costhe;
@@ -924,7 +927,7 @@ __device__ void annih(const DevCtx &C, Part p, Rng &r)
         p.e = esg2;
         costhe = fminf_(1.0f, (esg2 - rm) * pot / esg2);
         sinthe = -sqrtf(1.0f - costhe * costhe);
-        if (sinpsi >= 1e-10f) {
+        if (sinpsi >= 1e-10) {
             float us = sinthe * cphi, vs = sinthe * sphi;
             p.u = cc * cosdel * us - sindel * vs + aa * costhe;
             p.v = cc * sindel * us + cosdel * vs + bb * costhe;

@@ -300,7 +300,7 @@ __device__ uint32_t howfar_mlc(const DevCtx &C, Part &p0, float &t)
     bool to_new_region = false;
     if (inside_XZ && inside_YZ) {
         p3.x = p1.x + dis_xz * dir1.x;
-        p3.y = p1.y + (dis_xz - 0.001f) * dir1.y;
+        p3.y = p1.y + (dis_xz - 0.001) * dir1.y;   // in double, as geom.cu:591
         indexLimit1 = index_of_leaf(C, p3);
         if (indexLimit1 < 0) indexLimit1 = -indexLimit1;
     } else {

@@ -38,7 +38,8 @@ __device__ __forceinline__ void rotate_dir(float costhe, float sinthe, float cos
 __device__ __forceinline__ void uphi21(const DevCtx &C, float costhe, float sinthe, float &cosphi, float &sinphi, Part &p, Rng &r)
 {
     float r1 = U(C, r);
-    gx_sincos_turns(r1, &sinphi, &cosphi);
+    float phi = 2.0f * 3.14159265f * r1;      // utility.cu:99-100
+    gx_sincos(phi, &sinphi, &cosphi);
     rotate_dir(costhe, sinthe, cosphi, sinphi, p);
 }
 
@@ -48,9 +49,10 @@ __device__ __forceinline__ void uphi32(float costhe, float sinthe, float cosphi,
     rotate_dir(costhe, sinthe, cosphi, sinphi, p);
 }
 
-__device__ __forceinline__ void box_phi(const DevCtx &C, Rng &r, float &cphi, float &sphi)
+// a point of the unit disc by rejection; returns 1 / (x^2 + y^2)
+__device__ __forceinline__ float box_xy(const DevCtx &C, Rng &r, float &xphi, float &yphi)
 {
-    float xphi, yphi, rhophi2;
+    float rhophi2;
     int n = 0;
     do {
         xphi = U(C, r);
@@ -58,11 +60,19 @@ __device__ __forceinline__ void box_phi(const DevCtx &C, Rng &r, float &cphi, fl
         yphi = U(C, r);
         rhophi2 = xphi * xphi + yphi * yphi;
     } while (rhophi2 > 1.0f && ++n < GX_LOOP_CAP);
-    rhophi2 = 1.0f / rhophi2;
+    return 1.0f / rhophi2;
+}
+
+__device__ __forceinline__ void box_phi(const DevCtx &C, Rng &r, float &cphi, float &sphi)
+{
+    float xphi, yphi;
+    const float rhophi2 = box_xy(C, r, xphi, yphi);
     cphi = (xphi * xphi - yphi * yphi) * rhophi2;
     sphi = 2.0f * xphi * yphi * rhophi2;
 }
 
+// isotropic direction of a fluorescence or Auger particle (relax.cu:187-217;
+// the products in the reference's order: sin(theta) times the box terms first)
 __device__ __forceinline__ void relax_direction(const DevCtx &C, Rng &r, Part &p)
 {
     float eta = U(C, r);
@@ -71,10 +81,10 @@ __device__ __forceinline__ void relax_direction(const DevCtx &C, Rng &r, Part &p
     eta = (1.0f - eta) * (1.0f + eta);
     if (eta > 1E-20f) {
         eta = sqrtf(eta);
-        float cphi, sphi;
-        box_phi(C, r, cphi, sphi);
-        p.u = eta * cphi;
-        p.v = eta * sphi;
+        float xphi, yphi;
+        const float rhophi2 = box_xy(C, r, xphi, yphi);
+        p.u = eta * (xphi * xphi - yphi * yphi) * rhophi2;
+        p.v = eta * 2.0f * xphi * yphi * rhophi2;
     } else {
         p.u = 0.0f; p.v = 0.0f; p.w = 1.0f;
     }
@@ -261,7 +271,7 @@ __device__ void compton(const DevCtx &C, Part p, Rng &r)
             }
             jo = __ldg(&P->jo_array[j - 1]);
         }
-        float bro = 1.0f / broi, br, temp = 0.0f, sinthe = 0.0f, costhe;
+        float bro = 1.0 / broi, br, temp = 0.0f, sinthe = 0.0f, costhe;
         int br_loops = 0;
         do {
             if (ko > 2.0f) {
@@ -317,8 +327,8 @@ __device__ void compton(const DevCtx &C, Part p, Rng &r)
                 pzmax = 1.0f; af = 0.0f; fmax1 = 1.0f; fpz = 1.0f;
             } else {
                 float aux3 = 1.0f + 2.0f * jo * fabsf(pzmax);
-                float aux4 = 0.5f * (1.0f - aux3 * aux3);
-                fpz = 0.5f * gx_exp(aux4);
+                float aux4 = 0.5 * (1 - aux3 * aux3);
+                fpz = 0.5 * gx_exp(aux4);
                 af = qc * (1.0f + br * (br - costhe) / qc2);
                 if (af < 0.0f) {
                     if (pzmax > 0.0f) fpz = 1.0f - fpz;
@@ -330,14 +340,14 @@ __device__ void compton(const DevCtx &C, Part p, Rng &r)
                     af = 0.0f; fmax1 = 1.0f;
                 } else {
                     float fpz1;
-                    if (pzmax < -0.15f) { fmax1 = 1.0f - af * 0.15f; fpz1 = fpz * fmax1 * jo; }
-                    else if (pzmax < 0.15f) {
+                    if (pzmax < -0.15) { fmax1 = 1 - af * 0.15; fpz1 = fpz * fmax1 * jo; }
+                    else if (pzmax < 0.15) {
                         fmax1 = 1.0f + af * pzmax;
-                        aux3 = 1.0f / (1.0f + 0.33267252734f * aux3);
-                        aux4 = fpz * aux3 * (0.3480242f + aux3 * (-0.0958798f + aux3 * 0.7478556f)) + __ldg(&P->erfjo_array[j - 1]);
-                        if (pzmax > 0.0f) { fpz1 = (1.0f - fmax1 * fpz) * jo - 0.62665706866f * af * aux4; fpz = 1.0f - fpz; }
-                        else fpz1 = fmax1 * fpz * jo - 0.62665706866f * af * aux4;
-                    } else { fmax1 = 1.0f + af * 0.15f; fpz1 = (1.0f - fmax1 * fpz) * jo; fpz = 1.0f - fpz; }
+                        aux3 = 1 / (1 + 0.33267252734 * aux3);
+                        aux4 = fpz * aux3 * (0.3480242 + aux3 * (-0.0958798 + aux3 * 0.7478556)) + __ldg(&P->erfjo_array[j - 1]);
+                        if (pzmax > 0.0f) { fpz1 = (1 - fmax1 * fpz) * jo - 0.62665706866 * af * aux4; fpz = 1.0f - fpz; }
+                        else fpz1 = fmax1 * fpz * jo - 0.62665706866 * af * aux4;
+                    } else { fmax1 = 1 + af * 0.15; fpz1 = (1.0f - fmax1 * fpz) * jo; fpz = 1.0f - fpz; }
                     float eta_incoh = U(C, r);
                     if (eta_incoh * jo > fpz1) {
                         if (ibcmpl == 1) { push_move(C, ST_PHOTON, p, r); break; }
@@ -351,29 +361,29 @@ __device__ void compton(const DevCtx &C, Part p, Rng &r)
                 if (ibcmpl != 2) {
                     float rnno18 = U(C, r);
                     rnno18 = rnno18 * fpz;
-                    if (rnno18 < 0.5f) {
-                        rnno18 = fmaxf_(1e-30f, 2.0f * rnno18);
-                        pz = 0.5f * (1.0f - sqrtf(1.0f - 2.0f * gx_log(rnno18))) / jo;
+                    if (rnno18 < 0.5) {
+                        rnno18 = fmax(1e-30, (double)(2.0f * rnno18));
+                        pz = 0.5 * (1 - sqrtf(1 - 2 * gx_log(rnno18))) / jo;
                     } else {
                         rnno18 = 2.0f * (1.0f - rnno18);
-                        pz = 0.5f * (sqrtf(1.0f - 2.0f * gx_log(rnno18)) - 1.0f) / jo;
+                        pz = 0.5 * (sqrtf(1 - 2 * gx_log(rnno18)) - 1) / jo;
                     }
                     if (fabsf(pz) > 1.0f) continue;
-                    if (pz < 0.15f) {
+                    if (pz < 0.15) {
                         float frej;
-                        if (pz < -0.15f) frej = 1.0f - af * 0.15f; else frej = 1.0f + af * pz;
+                        if (pz < -0.15) frej = 1 - af * 0.15; else frej = 1.0f + af * pz;
                         float eta = U(C, r);
                         if (eta * fmax1 > frej) continue;
                     }
                 } else { pz = 0.0f; uj = 0.0f; }
                 break;
             }
-            if (fabsf(pz) < 0.01f) br = br * (1.0f + pz * (qc + (br * br - costhe) * pz));
+            if (fabsf(pz) < 0.01) br = br * (1.0f + pz * (qc + (br * br - costhe) * pz));
             else {
                 float a1 = 1.0f - pz * pz * br * costhe;
                 float a2 = 1.0f - pz * pz * br * br;
                 float a3 = qc2 - br * br * pz * pz * sinthe;
-                if (a3 > 1e-10f) br = br / a2 * (a1 + pz * sqrtf(a3));
+                if (a3 > 1e-10) br = br / a2 * (a1 + pz * sqrtf(a3));
             }
             uj = uj * prm;
         }
@@ -386,7 +396,7 @@ __device__ void compton(const DevCtx &C, Part p, Rng &r)
         if (p.e < rd.pcut) edep += p.e;
         else push_spawn(C, ST_PHOTON, p, r);
         float aux = 1.0f + br * br - 2.0f * br * costhe;
-        if (aux > 1e-8f) {
+        if (aux > 1e-8) {
             costhe = (1.0f - br * costhe) / sqrtf(aux);
             sinthe = (1.0f - costhe) * (1.0f + costhe);
             if (sinthe > 0.0f) sinthe = -sqrtf(sinthe); else sinthe = 0.0f;
@@ -397,7 +407,7 @@ __device__ void compton(const DevCtx &C, Part p, Rng &r)
         if (p1.e < rd.ecut) edep += p1.e - prm;
         else push_spawn(C, ST_ELECTRON, p1, r);
         if ((ibcmpl == 1) || (ibcmpl == 3)) {
-            if (uj > 0.001f)
+            if (uj > 0.001)
                 relax(C, uj, __ldg(&P->shn_array[j - 1]), __ldg(&P->iz_array[j - 1]), edep, p, rd, r);
             else edep += uj;
         }
@@ -432,7 +442,7 @@ __device__ void photo(const DevCtx &C, Part p, Rng &r)
     if (iedgfl != 0) {
         int nne = P->nne[medium];
         if (nne == 1) {
-            iz = (int)(__ldg(&P->zelem[medium]) + 0.5f);
+            iz = (int)(__ldg(&P->zelem[medium]) + 0.5);
             for (j = 0; j < __ldg(&P->edge_number[iz - 1]); j++)
                 if (peig >= __ldg(&P->edge_energies[GEGS_MXEDGE * (iz - 1) + j])) break;
         } else {
@@ -441,7 +451,7 @@ __device__ void photo(const DevCtx &C, Part p, Rng &r)
             aux = aux * sqrtf(peig);
             float sigtot = 0.0f;
             for (k = 0; k < nne; k++) {
-                iz = (int)(__ldg(&P->zelem[GX_MXMED * k + medium]) + 0.5f);
+                iz = (int)(__ldg(&P->zelem[GX_MXMED * k + medium]) + 0.5);
                 int b = GEGS_MXEDGE * (iz - 1);
                 float sigma;
                 if (peig > __ldg(&P->edge_energies[b])) {
@@ -466,7 +476,7 @@ __device__ void photo(const DevCtx &C, Part p, Rng &r)
                 if (br <= 0.0f) break;
             }
             if (k >= nne) k = nne - 1;
-            iz = (int)(__ldg(&P->zelem[GX_MXMED * k + medium]) + 0.5f);
+            iz = (int)(__ldg(&P->zelem[GX_MXMED * k + medium]) + 0.5);
             j = ints[k];
         }
         if (peig <= __ldg(&P->binding_energies[GEGS_MXSHELL * (iz - 1) + 5])) {
@@ -494,15 +504,15 @@ __device__ void photo(const DevCtx &C, Part p, Rng &r)
             if (iphter) {
                 float beta = sqrtf((p.e - rm) * (p.e + rm)) / p.e;
                 float gamma = p.e / rm;
-                float alpha = 0.5f * gamma - 0.5f + 1.0f / gamma;
+                float alpha = 0.5 * gamma - 0.5 + 1.0f / gamma;
                 float ratio = beta / alpha;
                 float xi, rnpht2, sinth2, costhe;
                 int nl = 0;
                 do {
                     float rnpht = U(C, r);
                     rnpht = 2.0f * rnpht - 1.0f;
-                    if (ratio <= 0.2f) {
-                        float fkappa = rnpht + 0.5f * ratio * (1.0f - rnpht) * (1.0f + rnpht);
+                    if (ratio <= 0.2) {
+                        float fkappa = rnpht + 0.5 * ratio * (1.0f - rnpht) * (1 + rnpht);
                         if (gamma < 100.0f) costhe = (beta + fkappa) / (1.0f + beta * fkappa);
                         else {
                             if (fkappa > 0.0f)
@@ -516,7 +526,7 @@ __device__ void photo(const DevCtx &C, Part p, Rng &r)
                     }
                     sinth2 = fmaxf_(0.0f, (1.0f - costhe) * (1.0f + costhe));
                     rnpht2 = U(C, r);
-                } while (rnpht2 > (0.5f * (1.0f + gamma) * sinth2 * xi / gamma) && ++nl < GX_LOOP_CAP);
+                } while (rnpht2 > (0.5 * (1.0f + gamma) * sinth2 * xi / gamma) && ++nl < GX_LOOP_CAP);
                 float sinthe = sqrtf(sinth2);
                 float sinphi, cosphi;
                 uphi21(C, costhe, sinthe, cosphi, sinphi, p, r);
@@ -612,7 +622,7 @@ __device__ void pair_angle(const DevCtx &C, Rng &r, int use, float ese, float ei
     if (use == 1) {
         float pse = sqrtf(fmaxf_(0.0f, (ese - rm) * (ese + rm)));
         float c = U(C, r);
-        c = 1.0f - 2.0f * c;
+        c = 1.0f - 2.0 * c;
         sinthe = rm * sqrtf((1.0f - c) * (1.0f + c)) / (pse * c + ese);
         costhe = (ese * c + pse) / (pse * c + ese);
     } else if (use == 2) {
@@ -620,28 +630,28 @@ __device__ void pair_angle(const DevCtx &C, Rng &r, int use, float ese, float ei
         float tteig = eig / rm, ttese = ese / rm;
         float esedei = ttese / (tteig - ttese);
         float eseder = 1.0f / esedei;
-        float ximin = 1.0f / (1.0f + (3.141593f * ttese) * (3.141593f * ttese));
+        float ximin = 1.0f / (1.0f + (3.141593 * ttese) * (3.141593 * ttese));
         float g1 = ((1.0f + eseder) * (1.0f + esedei) / (2.0f * tteig));
-        float rejmin = 2.0f + 3.0f * (esedei + eseder) - 4.0f * (esedei + eseder + 1.0f - 4.0f * (ximin - 0.5f) * (ximin - 0.5f))
+        float rejmin = 2.0f + 3.0f * (esedei + eseder) - 4.00 * (esedei + eseder + 1.0f - 4.0f * (ximin - 0.5f) * (ximin - 0.5f))
                        * (1.0f + 0.25f * gx_log(g1 * g1 + ztarg * ximin * ximin));
         float ya = (2.0f / tteig) * (2.0f / tteig);
         float xitry = fmaxf_(0.01f, fmaxf_(ximin, fminf_(0.5f, sqrtf(ya / ztarg))));
-        float galpha = 1.0f + 0.25f * gx_log(ya + ztarg * xitry * xitry);
+        float galpha = 1.0f + 0.25 * gx_log(ya + ztarg * xitry * xitry);
         float gbeta = 0.5f * ztarg * xitry / (ya + ztarg * xitry * xitry);
         galpha = galpha - gbeta * (xitry - 0.5f);
         float ximid = galpha / (3.0f * gbeta);
-        if (galpha >= 0.0f) ximid = 0.5f - ximid + sqrtf(ximid * ximid + 0.25f);
-        else ximid = 0.5f - ximid - sqrtf(ximid * ximid + 0.25f);
+        if (galpha >= 0.0f) ximid = 0.5f - ximid + sqrtf(ximid * ximid + 0.25);
+        else ximid = 0.5f - ximid - sqrtf(ximid * ximid + 0.25);
         ximid = fmaxf_(0.01f, fmaxf_(ximin, fminf_(0.5f, ximid)));
-        float rejmid = 2.0f + 3.0f * (esedei + eseder) - 4.0f * (esedei + eseder + 1.0f - 4.0f * (ximid - 0.5f) * (ximid - 0.5f))
-                       * (1.0f + 0.25f * gx_log(g1 * g1 + ztarg * ximid * ximid));
-        float rejtop = 1.02f * fmaxf_(rejmin, rejmid);
+        float rejmid = 2.0f + 3.0f * (esedei + eseder) - 4.0f * (esedei + eseder + 1.0f - 4.0 * (ximid - 0.5f) * (ximid - 0.5f))
+                       * (1.0f + 0.25 * gx_log(g1 * g1 + ztarg * ximid * ximid));
+        float rejtop = 1.02 * fmaxf_(rejmin, rejmid);
         float rtest, rtst, theta;
         int n = 0;
         do {
             float xitst = U(C, r);
-            float rejtst = 2.0f + 3.0f * (esedei + eseder) - 4.0f * (esedei + eseder + 1.0f - 4.0f * (xitst - 0.5f) * (xitst - 0.5f))
-                           * (1.0f + 0.25f * gx_log(g1 * g1 + ztarg * xitst * xitst));
+            float rejtst = 2.0f + 3.0f * (esedei + eseder) - 4.0f * (esedei + eseder + 1.0f - 4.0f * (xitst - 0.5) * (xitst - 0.5))
+                           * (1.0f + 0.25 * gx_log(g1 * g1 + ztarg * xitst * xitst));
             rtest = U(C, r);
             theta = sqrtf(1.0f / xitst - 1.0f) / ttese;
             rtst = rejtst / rejtop;
@@ -673,12 +683,12 @@ __device__ void pair(const DevCtx &C, Part p, Rng &r)
     float eig = p.e;
     float ese1, ese2;
     int iq1, iq2;
-    if (eig <= 2.1f) {
+    if (eig <= 2.1) {
         float rnno30 = U(C, r);
-        ese2 = prm + 0.5f * rnno30 * (eig - 2.0f * prm);
+        ese2 = prm + 0.5 * rnno30 * (eig - 2 * prm);
         rnno30 = U(C, r);
         ese1 = eig - ese2;
-        if (rnno30 < 0.5f) { iq1 = -1; iq2 = 1; } else { iq1 = 1; iq2 = -1; }
+        if (rnno30 < 0.5) { iq1 = -1; iq2 = 1; } else { iq1 = 1; iq2 = -1; }
     } else {
         float amax, bmax, aux1;
         int l, l1;
@@ -711,13 +721,13 @@ __device__ void pair(const DevCtx &C, Part p, Rng &r)
             rnno30 = U(C, r);
             float rnno31 = U(C, r);
             float br;
-            if (rnno30 > aux1) { br = 0.5f * rnno31; rejmax = bmax; l1 = l + 1; }
+            if (rnno30 > aux1) { br = 0.5 * rnno31; rejmax = bmax; l1 = l + 1; }
             else {
                 rnno30 = U(C, r);
                 rnno30 = fmaxf_(rnno30, rnno31);
                 rnno31 = U(C, r);
                 float b1 = fmaxf_(rnno30, rnno31);
-                br = 0.5f * (1.0f - b1);
+                br = 0.5 * (1 - b1);
                 rejmax = amax;
                 l1 = l;
             }
@@ -733,7 +743,7 @@ __device__ void pair(const DevCtx &C, Part p, Rng &r)
         ese2 = eminus;
         ese1 = eig - ese2;
         rnno30 = U(C, r);
-        if (rnno30 < 0.5f) { iq1 = -1; iq2 = 1; } else { iq1 = 1; iq2 = -1; }
+        if (rnno30 < 0.5) { iq1 = -1; iq2 = 1; } else { iq1 = 1; iq2 = -1; }
     }
     p.e = ese1;
     p1.e = ese2;
@@ -747,7 +757,7 @@ __device__ void pair(const DevCtx &C, Part p, Rng &r)
             float rtest = U(C, r);
             float gbeta = ese1 / (ese1 + 10.0f);
             use = (rtest < gbeta) ? 1 : 4;
-        } else if ((iprdst == 2) && (eig < 4.14f)) use = 1;
+        } else if ((iprdst == 2) && (eig < 4.14)) use = 1;
         else use = iprdst;
         for (int ichrg = 1; ichrg <= 2; ichrg++) {
             float ese;
@@ -782,7 +792,8 @@ __device__ void pair(const DevCtx &C, Part p, Rng &r)
     {
         float r1 = U(C, r);
         gx_sincos(0.0f, &sinthe, &costhe);
-        gx_sincos_turns(r1, &sinphi, &cosphi);
+        float phi = 2.0f * 3.14159265f * r1;  // uphi11 (utility.cu:190-191)
+        gx_sincos(phi, &sinphi, &cosphi);
         rotate_dir(costhe, sinthe, cosphi, sinphi, p);
     }
     if (p.e < rd.ecut) {

@@ -51,7 +51,12 @@ uint32_t ora_rng_u32(ora_ctx *C, ora_rng *r)
 float ora_rng_uniform(ora_ctx *C, ora_rng *r)
 {
     uint32_t x = ora_rng_u32(C, r);
-    return (float)((x >> 8) + 1u) * 5.9604644775390625e-08f;   /* 2^-24 */
+    float u = (float)((x >> 8) + 1u) * 5.9604644775390625e-08f;   /* 2^-24 */
+    if (C && C->urec) {
+        if (C->urec_n < C->urec_cap) C->urec[C->urec_n] = u;
+        C->urec_n++;
+    }
+    return u;
 }
 
 void ora_rng_spawn(ora_ctx *C, ora_rng *parent, ora_rng *child)
@@ -148,6 +153,10 @@ void gx_sincos(float a, float *s, float *c)
 /* ---- scoring (scoring.cu:14-26) with an int64 fixed-point tally ---------- */
 void ora_escore(ora_ctx *C, uint32_t region, float energy)
 {
+    if (C->drec_region) {
+        if (C->drec_n < C->drec_cap) { C->drec_region[C->drec_n] = region; C->drec_e[C->drec_n] = energy; }
+        C->drec_n++;
+    }
     if (region < VAC_AND_OTH) { C->e_escaped += (double)energy; return; }
     C->cnt[C->cur_stage][1]++;
     C->tally[region - VAC_AND_OTH] += (int64_t)llrintf(energy * 1073741824.0f);
@@ -209,7 +218,8 @@ static void rotate(float costhe, float sinthe, float cosphi, float sinphi, ora_p
 void uphi21(ora_ctx *C, float costhe, float sinthe, float *cosphi, float *sinphi, ora_particle *p, ora_rng *r)
 {
     float r1 = ora_rng_uniform(C, r);
-    gx_sincos_turns(r1, sinphi, cosphi);
+    float phi = 2.0f * 3.14159265f * r1;              /* utility.cu:99-100 */
+    gx_sincos(phi, sinphi, cosphi);
     rotate(costhe, sinthe, *cosphi, *sinphi, p);
 }
 
@@ -222,6 +232,7 @@ void uphi11(ora_ctx *C, float theta, float *costhe, float *sinthe, float *cosphi
 {
     float r1 = ora_rng_uniform(C, r);
     gx_sincos(theta, sinthe, costhe);
-    gx_sincos_turns(r1, sinphi, cosphi);
+    float phi = 2.0f * 3.14159265f * r1;              /* utility.cu:190-191 */
+    gx_sincos(phi, sinphi, cosphi);
     rotate(*costhe, *sinthe, *cosphi, *sinphi, p);
 }

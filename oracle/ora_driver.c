@@ -22,7 +22,7 @@ uint32_t ora_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t
     return ora_philox_word(c0, c1, c2, c3, k0, k1, lane);
 }
 
-static ora_region *build_regions(const gegs_physics *P, const gegs_scene *S, uint32_t nvox)
+ora_region *ora_build_regions(const gegs_physics *P, const gegs_scene *S, uint32_t nvox)
 {
     ora_region *reg = (ora_region *)calloc((size_t)nvox + VAC_AND_OTH, sizeof(ora_region));
     reg[0].med = VACUUM;
@@ -49,7 +49,7 @@ static ora_region *build_regions(const gegs_physics *P, const gegs_scene *S, uin
 }
 
 /* history index -> primary particle (CUDA_EGS.cu:52-131) */
-static int make_primary(const gegs_scene *S, uint64_t h, ora_particle *p)
+int ora_make_primary(const gegs_scene *S, uint64_t h, ora_particle *p)
 {
     int f;
     for (f = 0; f < S->nfields; f++)
@@ -99,7 +99,7 @@ static int make_primary(const gegs_scene *S, uint64_t h, ora_particle *p)
     return 1;
 }
 
-static void run_particle(ora_ctx *C, ora_particle *p)
+void ora_run_particle(ora_ctx *C, ora_particle *p)
 {
     C->counts[p->status]++;
     C->cur_stage = p->status;
@@ -130,7 +130,7 @@ int ora_run(const gegs_physics *P, const gegs_scene *S, uint64_t h0, uint64_t h1
 {
     if (g_trace) nthreads = 1;
     uint32_t nvox = (uint32_t)S->nx * (uint32_t)S->ny * (uint32_t)S->nz;
-    ora_region *reg = build_regions(P, S, nvox);
+    ora_region *reg = ora_build_regions(P, S, nvox);
     ora_stats tot;
     memset(&tot, 0, sizeof(tot));
 #ifdef _OPENMP
@@ -159,12 +159,12 @@ int ora_run(const gegs_physics *P, const gegs_scene *S, uint64_t h0, uint64_t h1
 #pragma omp for schedule(dynamic, 64)
         for (int64_t h = (int64_t)h0; h < (int64_t)h1; h++) {
             ora_particle p;
-            if (!make_primary(S, (uint64_t)h, &p)) { C.error |= 4; continue; }
+            if (!ora_make_primary(S, (uint64_t)h, &p)) { C.error |= 4; continue; }
             stk.n = 0;
             ora_push(&C, &p, p.status);
             while (stk.n > 0) {
                 ora_particle q = stk.a[--stk.n];
-                run_particle(&C, &q);
+                ora_run_particle(&C, &q);
             }
         }
 #pragma omp critical

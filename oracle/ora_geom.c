@@ -274,7 +274,7 @@ static uint32_t howfar_MLC(ora_ctx *C, ora_particle *p0, float *t)
     if (dis_xz < dis_yz) minBoundaryDist = dis_xz; else minBoundaryDist = dis_yz;
     if (inside_XZ && inside_YZ) {
         p3.x = p1.x + dis_xz * dir1.x;
-        p3.y = p1.y + (dis_xz - 0.001f) * dir1.y;
+        p3.y = p1.y + (dis_xz - 0.001) * dir1.y;
         indexLimit1 = indexOfLeaf(S, p3);
         if (indexLimit1 < 0) indexLimit1 = -indexLimit1;
     } else {
@@ -467,7 +467,7 @@ static float pointDistToSegment(pt2 p, pt2 v, pt2 w)
 
 static float pointMinDistToPolygon(pt2 p0, const float (*poly)[2], int n)
 {
-    float minDist = 1e9f;
+    float minDist = 1e9;
     for (int i = 0; i < n; i++) {
         int j = i + 1;
         if (j >= n) j = 0;

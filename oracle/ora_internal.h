@@ -45,20 +45,23 @@
 #define MAXU_MS GEGS_MAXU_MS
 #define MAXL_MS_PLUS_1 (MAXL_MS + 1)
 #define MAXQ_MS_PLUS_1 (MAXQ_MS + 1)
-#define LAMBMAX_MS 1e5f
-#define QMIN_MS 1e-3f
-#define QMAX_MS 0.5f
+#define LAMBMAX_MS 1e5
+#define QMIN_MS 1e-3
+#define QMAX_MS 0.5
 #define MXVAC 10
-#define RELAX_CUTOFF 0.001f
-#define EPSEMFP 1.e-5f
-#define EPSGMFP 1.e-5f
-#define EPSTEP 0.0005f
-#define INFI_DIST 1e5f
+#define RELAX_CUTOFF 0.001
+#define EPSEMFP 1.e-5
+#define EPSGMFP 1.e-5
+#define EPSTEP 0.0005
+#define INFI_DIST 1e5
 #define OUTMLC (-99)
 #define PASSMLC (-98)
 #define VACUUM 0xFFFFu
 #define VACUUM_STEP 1E8f
 #define SMALL_POLAR_ANGLE_THRESHOLD 1E-20f
+/* The reference's constants keep its types: these are double literals
+ * (EGSnrc_Parameters.h:78-127, CUDA_EGS.h:34,80), so an expression that uses
+ * one is evaluated in double, as in the reference. */
 #define HC_INVERSE 80.65506856998f
 #define TWICE_HC2 0.000307444456f
 #define PRESTA_II 0
@@ -126,6 +129,12 @@ typedef struct {
     int cur_stage;
     ora_trace_rec *trace;    /* debug trace (single-threaded runs only) */
     uint32_t trace_n, trace_cap;
+    /* probes: record every uniform drawn and every escore call (null: off) */
+    float *urec;
+    uint32_t urec_n, urec_cap;
+    uint32_t *drec_region;
+    float *drec_e;
+    uint32_t drec_n, drec_cap;
 } ora_ctx;
 
 void ora_trace(ora_ctx *C, uint32_t kind, int stage, const ora_particle *p);
@@ -148,6 +157,11 @@ void ora_spawn(ora_ctx *C, ora_rng *parent, ora_particle *child, int status);
 void uphi21(ora_ctx *C, float costhe, float sinthe, float *cosphi, float *sinphi, ora_particle *p, ora_rng *r);
 void uphi32(float costhe, float sinthe, float cosphi, float sinphi, ora_particle *p);
 void uphi11(ora_ctx *C, float theta, float *costhe, float *sinthe, float *cosphi, float *sinphi, ora_particle *p, ora_rng *r);
+
+/* driver (ora_driver.c) */
+ora_region *ora_build_regions(const gegs_physics *P, const gegs_scene *S, uint32_t nvox);
+void ora_run_particle(ora_ctx *C, ora_particle *p);
+int ora_make_primary(const gegs_scene *S, uint64_t h, ora_particle *p);
 
 /* geometry (ora_geom.c) */
 uint32_t ora_howfar(ora_ctx *C, ora_particle *p, float *t, int *ok);

@@ -19,23 +19,31 @@ static const short final_state[39] = {4, 3, 5, 6, 202, 302, 402, 404, 403, 303, 
 
 static inline float U(ora_ctx *C, ora_rng *r) { return ora_rng_uniform(C, r); }
 
+/* a point of the unit disc by rejection; returns 1 / (x^2 + y^2) */
+static float box_xy(ora_ctx *C, ora_rng *r, float *xphi, float *yphi)
+{
+    float rhophi2;
+    int n = 0;
+    do {
+        *xphi = U(C, r);
+        *xphi = 2.0f * *xphi - 1.0f;
+        *yphi = U(C, r);
+        rhophi2 = *xphi * *xphi + *yphi * *yphi;
+    } while (rhophi2 > 1.0f && ++n < ORA_LOOP_CAP);
+    return 1.0f / rhophi2;
+}
+
 /* azimuth by the box method ($SELECT-AZIMUTHAL-ANGLE) */
 static void box_phi(ora_ctx *C, ora_rng *r, float *cphi, float *sphi)
 {
-    float xphi, yphi, rhophi2;
-    int n = 0;
-    do {
-        xphi = U(C, r);
-        xphi = 2.0f * xphi - 1.0f;
-        yphi = U(C, r);
-        rhophi2 = xphi * xphi + yphi * yphi;
-    } while (rhophi2 > 1.0f && ++n < ORA_LOOP_CAP);
-    rhophi2 = 1.0f / rhophi2;
+    float xphi, yphi;
+    float rhophi2 = box_xy(C, r, &xphi, &yphi);
     *cphi = (xphi * xphi - yphi * yphi) * rhophi2;
     *sphi = 2.0f * xphi * yphi * rhophi2;
 }
 
-/* isotropic direction used by RELAX for fluorescence/Auger particles */
+/* isotropic direction used by RELAX for fluorescence/Auger particles
+ * (relax.cu:187-217; products in the reference's order) */
 static void relax_direction(ora_ctx *C, ora_rng *r, ora_particle *p)
 {
     float eta = U(C, r);
@@ -44,10 +52,10 @@ static void relax_direction(ora_ctx *C, ora_rng *r, ora_particle *p)
     eta = (1.0f - eta) * (1.0f + eta);
     if (eta > SMALL_POLAR_ANGLE_THRESHOLD) {
         eta = sqrtf(eta);
-        float cphi, sphi;
-        box_phi(C, r, &cphi, &sphi);
-        p->u = eta * cphi;
-        p->v = eta * sphi;
+        float xphi, yphi;
+        float rhophi2 = box_xy(C, r, &xphi, &yphi);
+        p->u = eta * (xphi * xphi - yphi * yphi) * rhophi2;
+        p->v = eta * 2.0f * xphi * yphi * rhophi2;
     } else {
         p->u = 0.0f; p->v = 0.0f; p->w = 1.0f;
     }
@@ -233,7 +241,7 @@ void ora_compton(ora_ctx *C, ora_particle *p)
             jo = P->jo_array[j - 1];
         }
         /* Klein-Nishina (always); alph1/alpha/bro/rejmax recomputed every pass */
-        float bro = 1.0f / broi, br, temp = 0.0f, sinthe = 0.0f, costhe;
+        float bro = 1.0 / broi, br, temp = 0.0f, sinthe = 0.0f, costhe;
         int br_loops = 0;
         do {
             if (ko > 2.0f) {
@@ -289,8 +297,8 @@ void ora_compton(ora_ctx *C, ora_particle *p)
                 pzmax = 1.0f; af = 0.0f; fmax1 = 1.0f; fpz = 1.0f;
             } else {
                 float aux3 = 1.0f + 2.0f * jo * fabsf(pzmax);
-                float aux4 = 0.5f * (1.0f - aux3 * aux3);
-                fpz = 0.5f * gx_exp(aux4);
+                float aux4 = 0.5 * (1 - aux3 * aux3);
+                fpz = 0.5 * gx_exp(aux4);
                 af = qc * (1.0f + br * (br - costhe) / qc2);
                 if (af < 0.0f) {
                     if (pzmax > 0.0f) fpz = 1.0f - fpz;
@@ -302,14 +310,14 @@ void ora_compton(ora_ctx *C, ora_particle *p)
                     af = 0.0f; fmax1 = 1.0f;
                 } else {
                     float fpz1;
-                    if (pzmax < -0.15f) { fmax1 = 1.0f - af * 0.15f; fpz1 = fpz * fmax1 * jo; }
-                    else if (pzmax < 0.15f) {
+                    if (pzmax < -0.15) { fmax1 = 1 - af * 0.15; fpz1 = fpz * fmax1 * jo; }
+                    else if (pzmax < 0.15) {
                         fmax1 = 1.0f + af * pzmax;
-                        aux3 = 1.0f / (1.0f + 0.33267252734f * aux3);
-                        aux4 = fpz * aux3 * (0.3480242f + aux3 * (-0.0958798f + aux3 * 0.7478556f)) + P->erfjo_array[j - 1];
-                        if (pzmax > 0.0f) { fpz1 = (1.0f - fmax1 * fpz) * jo - 0.62665706866f * af * aux4; fpz = 1.0f - fpz; }
-                        else fpz1 = fmax1 * fpz * jo - 0.62665706866f * af * aux4;
-                    } else { fmax1 = 1.0f + af * 0.15f; fpz1 = (1.0f - fmax1 * fpz) * jo; fpz = 1.0f - fpz; }
+                        aux3 = 1 / (1 + 0.33267252734 * aux3);
+                        aux4 = fpz * aux3 * (0.3480242 + aux3 * (-0.0958798 + aux3 * 0.7478556)) + P->erfjo_array[j - 1];
+                        if (pzmax > 0.0f) { fpz1 = (1 - fmax1 * fpz) * jo - 0.62665706866 * af * aux4; fpz = 1.0f - fpz; }
+                        else fpz1 = fmax1 * fpz * jo - 0.62665706866 * af * aux4;
+                    } else { fmax1 = 1 + af * 0.15; fpz1 = (1.0f - fmax1 * fpz) * jo; fpz = 1.0f - fpz; }
                     float eta_incoh = U(C, &r);
                     if (eta_incoh * jo > fpz1) {
                         if (ibcmpl == 1) { p->rng = r; ora_push(C, p, p_photon_step); break; }
@@ -323,29 +331,29 @@ void ora_compton(ora_ctx *C, ora_particle *p)
                 if (ibcmpl != 2) {
                     float rnno18 = U(C, &r);
                     rnno18 = rnno18 * fpz;
-                    if (rnno18 < 0.5f) {
-                        rnno18 = fmaxf_(1e-30f, 2.0f * rnno18);
-                        pz = 0.5f * (1.0f - sqrtf(1.0f - 2.0f * gx_log(rnno18))) / jo;
+                    if (rnno18 < 0.5) {
+                        rnno18 = fmax(1e-30, (double)(2.0f * rnno18));
+                        pz = 0.5 * (1 - sqrtf(1 - 2 * gx_log(rnno18))) / jo;
                     } else {
                         rnno18 = 2.0f * (1.0f - rnno18);
-                        pz = 0.5f * (sqrtf(1.0f - 2.0f * gx_log(rnno18)) - 1.0f) / jo;
+                        pz = 0.5 * (sqrtf(1 - 2 * gx_log(rnno18)) - 1) / jo;
                     }
                     if (fabsf(pz) > 1.0f) continue;
-                    if (pz < 0.15f) {
+                    if (pz < 0.15) {
                         float frej;
-                        if (pz < -0.15f) frej = 1.0f - af * 0.15f; else frej = 1.0f + af * pz;
+                        if (pz < -0.15) frej = 1 - af * 0.15; else frej = 1.0f + af * pz;
                         float eta = U(C, &r);
                         if (eta * fmax1 > frej) continue;
                     }
                 } else { pz = 0.0f; uj = 0.0f; }
                 break;
             }
-            if (fabsf(pz) < 0.01f) br = br * (1.0f + pz * (qc + (br * br - costhe) * pz));
+            if (fabsf(pz) < 0.01) br = br * (1.0f + pz * (qc + (br * br - costhe) * pz));
             else {
                 float a1 = 1.0f - pz * pz * br * costhe;
                 float a2 = 1.0f - pz * pz * br * br;
                 float a3 = qc2 - br * br * pz * pz * sinthe;
-                if (a3 > 1e-10f) br = br / a2 * (a1 + pz * sqrtf(a3));
+                if (a3 > 1e-10) br = br / a2 * (a1 + pz * sqrtf(a3));
             }
             uj = uj * prm;
         }
@@ -358,7 +366,7 @@ void ora_compton(ora_ctx *C, ora_particle *p)
         if (p->e < rd->pcut) edep += p->e;
         else ora_spawn(C, &r, p, p_photon_step);
         float aux = 1.0f + br * br - 2.0f * br * costhe;
-        if (aux > 1e-8f) {
+        if (aux > 1e-8) {
             costhe = (1.0f - br * costhe) / sqrtf(aux);
             sinthe = (1.0f - costhe) * (1.0f + costhe);
             if (sinthe > 0.0f) sinthe = -sqrtf(sinthe); else sinthe = 0.0f;
@@ -405,7 +413,7 @@ void ora_photo(ora_ctx *C, ora_particle *p)
     if (iedgfl != 0) {
         int nne = P->nne[medium];
         if (nne == 1) {
-            iz = (int)(P->zelem[medium] + 0.5f);
+            iz = (int)(P->zelem[medium] + 0.5);
             for (j = 0; j < P->edge_number[iz - 1]; j++)
                 if (peig >= P->edge_energies[MXEDGE * (iz - 1) + j]) break;
         } else {
@@ -414,7 +422,7 @@ void ora_photo(ora_ctx *C, ora_particle *p)
             aux = aux * sqrtf(peig);
             float sigtot = 0.0f;
             for (k = 0; k < nne; k++) {
-                iz = (int)(P->zelem[MXMED * k + medium] + 0.5f);
+                iz = (int)(P->zelem[MXMED * k + medium] + 0.5);
                 int b = MXEDGE * (iz - 1);
                 float sigma;
                 if (peig > P->edge_energies[b]) {
@@ -438,7 +446,7 @@ void ora_photo(ora_ctx *C, ora_particle *p)
                 if (br <= 0.0f) break;
             }
             if (k >= nne) k = nne - 1;                  /* rounding left br > 0 */
-            iz = (int)(P->zelem[MXMED * k + medium] + 0.5f);
+            iz = (int)(P->zelem[MXMED * k + medium] + 0.5);
             j = ints[k];
         }
         if (peig <= P->binding_energies[MXSHELL * (iz - 1) + 5]) {
@@ -466,15 +474,15 @@ void ora_photo(ora_ctx *C, ora_particle *p)
             if (iphter) {
                 float beta = sqrtf((p->e - rm) * (p->e + rm)) / p->e;
                 float gamma = p->e / rm;
-                float alpha = 0.5f * gamma - 0.5f + 1.0f / gamma;
+                float alpha = 0.5 * gamma - 0.5 + 1.0f / gamma;
                 float ratio = beta / alpha;
                 float xi, rnpht2, sinth2, costhe;
                 int nl = 0;
                 do {
                     float rnpht = U(C, &r);
                     rnpht = 2.0f * rnpht - 1.0f;
-                    if (ratio <= 0.2f) {
-                        float fkappa = rnpht + 0.5f * ratio * (1.0f - rnpht) * (1.0f + rnpht);
+                    if (ratio <= 0.2) {
+                        float fkappa = rnpht + 0.5 * ratio * (1.0f - rnpht) * (1 + rnpht);
                         if (gamma < 100.0f) costhe = (beta + fkappa) / (1.0f + beta * fkappa);
                         else {
                             if (fkappa > 0.0f)
@@ -488,7 +496,7 @@ void ora_photo(ora_ctx *C, ora_particle *p)
                     }
                     sinth2 = fmaxf_(0.0f, (1.0f - costhe) * (1.0f + costhe));
                     rnpht2 = U(C, &r);
-                } while (rnpht2 > (0.5f * (1.0f + gamma) * sinth2 * xi / gamma) && ++nl < ORA_LOOP_CAP);
+                } while (rnpht2 > (0.5 * (1.0f + gamma) * sinth2 * xi / gamma) && ++nl < ORA_LOOP_CAP);
                 float sinthe = sqrtf(sinth2);
                 float sinphi, cosphi;
                 uphi21(C, costhe, sinthe, &cosphi, &sinphi, p, &r);
@@ -583,7 +591,7 @@ static void pair_angle(ora_ctx *C, ora_rng *r, int use, float ese, float eig, un
     if (use == 1) {
         float pse = sqrtf(fmaxf_(0.0f, (ese - rm) * (ese + rm)));
         float c = U(C, r);
-        c = 1.0f - 2.0f * c;
+        c = 1.0f - 2.0 * c;
         *sinthe = rm * sqrtf((1.0f - c) * (1.0f + c)) / (pse * c + ese);
         *costhe = (ese * c + pse) / (pse * c + ese);
     } else if (use == 2) {
@@ -591,28 +599,28 @@ static void pair_angle(ora_ctx *C, ora_rng *r, int use, float ese, float eig, un
         float tteig = eig / rm, ttese = ese / rm;
         float esedei = ttese / (tteig - ttese);
         float eseder = 1.0f / esedei;
-        float ximin = 1.0f / (1.0f + (3.141593f * ttese) * (3.141593f * ttese));
+        float ximin = 1.0f / (1.0f + (3.141593 * ttese) * (3.141593 * ttese));
         float g1 = ((1.0f + eseder) * (1.0f + esedei) / (2.0f * tteig));
-        float rejmin = 2.0f + 3.0f * (esedei + eseder) - 4.0f * (esedei + eseder + 1.0f - 4.0f * (ximin - 0.5f) * (ximin - 0.5f))
+        float rejmin = 2.0f + 3.0f * (esedei + eseder) - 4.00 * (esedei + eseder + 1.0f - 4.0f * (ximin - 0.5f) * (ximin - 0.5f))
                        * (1.0f + 0.25f * gx_log(g1 * g1 + ztarg * ximin * ximin));
         float ya = (2.0f / tteig) * (2.0f / tteig);
         float xitry = fmaxf_(0.01f, fmaxf_(ximin, fminf_(0.5f, sqrtf(ya / ztarg))));
-        float galpha = 1.0f + 0.25f * gx_log(ya + ztarg * xitry * xitry);
+        float galpha = 1.0f + 0.25 * gx_log(ya + ztarg * xitry * xitry);
         float gbeta = 0.5f * ztarg * xitry / (ya + ztarg * xitry * xitry);
         galpha = galpha - gbeta * (xitry - 0.5f);
         float ximid = galpha / (3.0f * gbeta);
-        if (galpha >= 0.0f) ximid = 0.5f - ximid + sqrtf(ximid * ximid + 0.25f);
-        else ximid = 0.5f - ximid - sqrtf(ximid * ximid + 0.25f);
+        if (galpha >= 0.0f) ximid = 0.5f - ximid + sqrtf(ximid * ximid + 0.25);
+        else ximid = 0.5f - ximid - sqrtf(ximid * ximid + 0.25);
         ximid = fmaxf_(0.01f, fmaxf_(ximin, fminf_(0.5f, ximid)));
-        float rejmid = 2.0f + 3.0f * (esedei + eseder) - 4.0f * (esedei + eseder + 1.0f - 4.0f * (ximid - 0.5f) * (ximid - 0.5f))
-                       * (1.0f + 0.25f * gx_log(g1 * g1 + ztarg * ximid * ximid));
-        float rejtop = 1.02f * fmaxf_(rejmin, rejmid);
+        float rejmid = 2.0f + 3.0f * (esedei + eseder) - 4.0f * (esedei + eseder + 1.0f - 4.0 * (ximid - 0.5f) * (ximid - 0.5f))
+                       * (1.0f + 0.25 * gx_log(g1 * g1 + ztarg * ximid * ximid));
+        float rejtop = 1.02 * fmaxf_(rejmin, rejmid);
         float rtest, rtst, theta;
         int n = 0;
         do {
             float xitst = U(C, r);
-            float rejtst = 2.0f + 3.0f * (esedei + eseder) - 4.0f * (esedei + eseder + 1.0f - 4.0f * (xitst - 0.5f) * (xitst - 0.5f))
-                           * (1.0f + 0.25f * gx_log(g1 * g1 + ztarg * xitst * xitst));
+            float rejtst = 2.0f + 3.0f * (esedei + eseder) - 4.0f * (esedei + eseder + 1.0f - 4.0f * (xitst - 0.5) * (xitst - 0.5))
+                           * (1.0f + 0.25 * gx_log(g1 * g1 + ztarg * xitst * xitst));
             rtest = U(C, r);
             theta = sqrtf(1.0f / xitst - 1.0f) / ttese;
             rtst = rejtst / rejtop;
@@ -645,12 +653,12 @@ void ora_pair(ora_ctx *C, ora_particle *p)
     float eig = p->e;
     float ese1, ese2;
     int iq1, iq2;
-    if (eig <= 2.1f) {
+    if (eig <= 2.1) {
         float rnno30 = U(C, &r);
-        ese2 = prm + 0.5f * rnno30 * (eig - 2.0f * prm);
+        ese2 = prm + 0.5 * rnno30 * (eig - 2 * prm);
         rnno30 = U(C, &r);
         ese1 = eig - ese2;
-        if (rnno30 < 0.5f) { iq1 = -1; iq2 = 1; } else { iq1 = 1; iq2 = -1; }
+        if (rnno30 < 0.5) { iq1 = -1; iq2 = 1; } else { iq1 = 1; iq2 = -1; }
     } else {
         float amax, bmax, aux1;
         int l, l1;
@@ -683,13 +691,13 @@ void ora_pair(ora_ctx *C, ora_particle *p)
             rnno30 = U(C, &r);
             float rnno31 = U(C, &r);
             float br;
-            if (rnno30 > aux1) { br = 0.5f * rnno31; rejmax = bmax; l1 = l + 1; }
+            if (rnno30 > aux1) { br = 0.5 * rnno31; rejmax = bmax; l1 = l + 1; }
             else {
                 rnno30 = U(C, &r);
                 rnno30 = fmaxf_(rnno30, rnno31);
                 rnno31 = U(C, &r);
                 float b1 = fmaxf_(rnno30, rnno31);
-                br = 0.5f * (1.0f - b1);
+                br = 0.5 * (1 - b1);
                 rejmax = amax;
                 l1 = l;
             }
@@ -705,7 +713,7 @@ void ora_pair(ora_ctx *C, ora_particle *p)
         ese2 = eminus;
         ese1 = eig - ese2;
         rnno30 = U(C, &r);
-        if (rnno30 < 0.5f) { iq1 = -1; iq2 = 1; } else { iq1 = 1; iq2 = -1; }
+        if (rnno30 < 0.5) { iq1 = -1; iq2 = 1; } else { iq1 = 1; iq2 = -1; }
     }
     p->e = ese1;
     p1.e = ese2;
@@ -719,7 +727,7 @@ void ora_pair(ora_ctx *C, ora_particle *p)
             float rtest = U(C, &r);
             float gbeta = ese1 / (ese1 + 10.0f);
             use = (rtest < gbeta) ? 1 : 4;
-        } else if ((iprdst == 2) && (eig < 4.14f)) use = 1;
+        } else if ((iprdst == 2) && (eig < 4.14)) use = 1;
         else use = iprdst;
         for (int ichrg = 1; ichrg <= 2; ichrg++) {
             float ese;
