@@ -91,6 +91,13 @@ struct gegs_engine {
 
     gegs_run_stats last{};
     bool in_flight = false;            // gegs_launch queued a run that gegs_wait has not finished
+
+    // batch statistics (gegs_stat_*): per voxel the sum and sum of squares of
+    // batch energies (MeV) and the tally at the last fold
+    double *d_stat_s1 = nullptr, *d_stat_s2 = nullptr;
+    unsigned long long *d_stat_snap = nullptr;
+    uint64_t stat_nvox = 0;
+    uint32_t stat_batches = 0;
 };
 
 static gegs_status cuda_fail(gegs_engine *e, cudaError_t c, const char *what)
@@ -193,6 +200,7 @@ void gegs_destroy(gegs_engine *e)
     cudaFree(e->d_fields); cudaFree(e->d_cross); cudaFree(e->d_jaw_lines); cudaFree(e->d_phsp); cudaFree(e->d_tally);
     cudaFree(e->d_err); cudaFree(e->d_stats); cudaFree(e->d_sched); cudaFree(e->d_qmeta);
     cudaFree(e->d_trace); cudaFree(e->d_trace_n);
+    cudaFree(e->d_stat_s1); cudaFree(e->d_stat_s2); cudaFree(e->d_stat_snap);
     for (int q = 0; q < GX_NQ; q++) cudaFree(e->d_qbuf[q]);
     for (int k = 0; k < GX_NESTATE; k++) cudaFree(e->d_estate[k]);
     if (e->ev0) cudaEventDestroy(e->ev0);
@@ -778,6 +786,59 @@ extern "C" gegs_status gegs_get_dose(gegs_engine *e, const float *voxel_mass, do
     cudaFreeAsync(d_mass, e->stream);
     cudaFreeAsync(d_out, e->stream);
     CK(cudaStreamSynchronize(e->stream), "dose sync");
+    return GEGS_OK;
+}
+
+// ---- batch statistics (CUDA_EGS.cu:817-876, on the device) ------------------
+extern "C" gegs_status gegs_stat_begin(gegs_engine *e)
+{
+    if (!e || !e->d_tally) return GEGS_ERR_ARG;
+    if (e->in_flight) { e->err = "a launched run has not been waited for (gegs_wait)"; return GEGS_ERR_ARG; }
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    if (e->stat_nvox != e->nvox) {
+        CK(realloc_dev(&e->d_stat_s1, (size_t)e->nvox), "batch statistics");
+        CK(realloc_dev(&e->d_stat_s2, (size_t)e->nvox), "batch statistics");
+        CK(realloc_dev(&e->d_stat_snap, (size_t)e->nvox), "batch statistics");
+        e->stat_nvox = e->nvox;
+    }
+    CK(cudaMemsetAsync(e->d_stat_s1, 0, e->nvox * sizeof(double), e->stream), "stat reset");
+    CK(cudaMemsetAsync(e->d_stat_s2, 0, e->nvox * sizeof(double), e->stream), "stat reset");
+    CK(cudaMemcpyAsync(e->d_stat_snap, e->d_tally, e->nvox * 8, cudaMemcpyDeviceToDevice, e->stream), "stat snapshot");
+    CK(cudaStreamSynchronize(e->stream), "stat sync");
+    e->stat_batches = 0;
+    return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_stat_fold(gegs_engine *e)
+{
+    if (!e || !e->d_stat_s1 || e->stat_nvox != e->nvox) { if (e) e->err = "gegs_stat_fold: no gegs_stat_begin"; return GEGS_ERR_ARG; }
+    if (e->in_flight) { e->err = "a launched run has not been waited for (gegs_wait)"; return GEGS_ERR_ARG; }
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    k_stat_fold<<<e->nsm * 8, 256, 0, e->stream>>>(e->d_tally, e->d_stat_snap, e->d_stat_s1, e->d_stat_s2, e->nvox);
+    CK(cudaGetLastError(), "stat fold");
+    CK(cudaStreamSynchronize(e->stream), "stat sync");
+    e->stat_batches++;
+    return GEGS_OK;
+}
+
+extern "C" gegs_status gegs_stat_get(gegs_engine *e, double *mean, double *rel_se, uint64_t nvox, uint32_t *nbatch)
+{
+    if (!e || !mean || !rel_se || !nbatch || nvox != e->nvox || !e->d_stat_s1 || e->stat_nvox != e->nvox)
+        return GEGS_ERR_ARG;
+    if (e->stat_batches < 2) { e->err = "gegs_stat_get: at least two folded batches are needed"; return GEGS_ERR_ARG; }
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    double *d_mean = nullptr, *d_rel = nullptr;
+    CK(cudaMallocAsync(&d_mean, nvox * 8, e->stream), "stat output");
+    CK(cudaMallocAsync(&d_rel, nvox * 8, e->stream), "stat output");
+    k_stat_final<<<e->nsm * 8, 256, 0, e->stream>>>(e->d_stat_s1, e->d_stat_s2, (double)e->stat_batches, d_mean, d_rel,
+                                                   nvox);
+    CK(cudaGetLastError(), "stat final");
+    CK(cudaMemcpyAsync(mean, d_mean, nvox * 8, cudaMemcpyDeviceToHost, e->stream), "stat D2H");
+    CK(cudaMemcpyAsync(rel_se, d_rel, nvox * 8, cudaMemcpyDeviceToHost, e->stream), "stat D2H");
+    cudaFreeAsync(d_mean, e->stream);
+    cudaFreeAsync(d_rel, e->stream);
+    CK(cudaStreamSynchronize(e->stream), "stat sync");
+    *nbatch = e->stat_batches;
     return GEGS_OK;
 }
 

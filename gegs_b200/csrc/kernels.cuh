@@ -529,3 +529,29 @@ __global__ void k_dose(const unsigned long long *tally, const float *mass, doubl
         out[i] = (double)(long long)tally[i] * 9.313225746154785e-10 / m * unit;
     }
 }
+
+// ---- batch statistics (the reference's GET_UNCERTAINTY, CUDA_EGS.cu:817-876) ----
+// One batch ends: x = tally gained since the last fold (MeV), S1 += x, S2 += x^2.
+__global__ void k_stat_fold(const unsigned long long *tally, unsigned long long *snap, double *s1, double *s2,
+                            uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long t = tally[i];
+        const double x = (double)(long long)(t - snap[i]) * 9.313225746154785e-10;
+        snap[i] = t;
+        s1[i] += x;
+        s2[i] += x * x;
+    }
+}
+
+// Batch mean and the relative standard error of the mean of n batches,
+// sqrt((S2/n - (S1/n)^2) / (n - 1)) / (S1/n) (0 where nothing was deposited).
+__global__ void k_stat_final(const double *s1, const double *s2, double n, double *mean, double *rel, uint64_t nv)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nv; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double m = s1[i] / n;
+        const double v = s2[i] / n - m * m;
+        mean[i] = m;
+        rel[i] = m > 0.0 ? sqrt((v > 0.0 ? v : 0.0) / (n - 1.0)) / m : 0.0;
+    }
+}

@@ -21,7 +21,7 @@ MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_set_timeline", "gegs_get_timeline", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
            "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_set_tally", "gegs_get_dose", "gegs_get_stats",
            "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version",
-           "gegs_check_physics"]
+           "gegs_check_physics", "gegs_stat_begin", "gegs_stat_fold", "gegs_stat_get"]
 
 
 TRACE_DTYPE = np.dtype([("kind_stage", "<u4"), ("hist_lo", "<u4"), ("sid_lo", "<u4"), ("sid_hi", "<u4"),
@@ -85,6 +85,9 @@ def load_library(path=None):
         getattr(L, f).restype = C.c_size_t
     L.gegs_version.restype = C.c_char_p
     L.gegs_check_physics.argtypes = [vp, C.c_char_p, C.c_size_t]
+    L.gegs_stat_begin.argtypes = [vp]
+    L.gegs_stat_fold.argtypes = [vp]
+    L.gegs_stat_get.argtypes = [vp, vp, vp, C.c_uint64, C.POINTER(C.c_uint32)]
     if path is None:
         _lib = L
     return L
@@ -230,6 +233,24 @@ class Engine:
         out = np.zeros(self.nvox, np.float64)
         self._check(self.L.gegs_get_dose(self.h, m.ctypes.data, dose_unit, out.ctypes.data, self.nvox))
         return out
+
+    # ---- batch statistics (the reference's batch uncertainty, on the device) ----
+    def stat_begin(self):
+        """Start a series of batches at the current tally."""
+        self._check(self.L.gegs_stat_begin(self.h))
+
+    def stat_fold(self):
+        """End a batch: what was deposited since the previous fold is one batch."""
+        self._check(self.L.gegs_stat_fold(self.h))
+
+    def stat_get(self):
+        """(batch-mean energy per voxel in MeV, relative standard error of the
+        mean per voxel, number of batches)."""
+        mean = np.zeros(self.nvox, np.float64)
+        rel = np.zeros(self.nvox, np.float64)
+        n = C.c_uint32()
+        self._check(self.L.gegs_stat_get(self.h, mean.ctypes.data, rel.ctypes.data, self.nvox, C.byref(n)))
+        return mean, rel, n.value
 
     def stats(self) -> dict:
         s = RunStats()

@@ -181,6 +181,18 @@ gegs_status gegs_get_dose(gegs_engine *e, const float *voxel_mass, double dose_u
 
 gegs_status gegs_get_stats(gegs_engine *e, gegs_run_stats *out);
 
+/* Batch statistics on the device, the reference's GET_UNCERTAINTY batch
+ * method (CUDA_EGS.cu:817-876, there on the host after every batch):
+ * gegs_stat_begin starts a series at the current tally; each gegs_stat_fold
+ * ends a batch -- the energy deposited since the previous fold is that batch's
+ * x_b per voxel, and S1 += x_b, S2 += x_b^2 in double. gegs_stat_get returns
+ * per voxel the batch mean S1/n (MeV) and the relative standard error of the
+ * mean, sqrt((S2/n - (S1/n)^2) / (n - 1)) / (S1/n), the reference's formula
+ * (0 where nothing was deposited); n >= 2 folds are needed. */
+gegs_status gegs_stat_begin(gegs_engine *e);
+gegs_status gegs_stat_fold(gegs_engine *e);
+gegs_status gegs_stat_get(gegs_engine *e, double *mean, double *rel_se, uint64_t nvox, uint32_t *nbatch);
+
 /* Device pointer of the tally (for callers that keep results in HBM). */
 gegs_status gegs_tally_device_ptr(gegs_engine *e, void **out);
 

@@ -115,3 +115,41 @@ def test_timed_mode_bit_exact(engine, oracle):
     _assert_same(gpu, ref)
     assert st["stage_launches"][0] == st["waves"] - 1 or st["stage_launches"][0] >= 1
     assert sum(st["stage_ms"]) > 0
+
+
+# ---- the configurations at their full geometry --------------------------------
+# The sizes above keep the oracle fast; these run the geometry the bench and
+# BASELINE configurations use -- C1 60^3 at 0.5 cm, C2 120^3 at 0.25 cm, C3
+# 256x256x120 at 1x1x2.5 mm (7.9M voxels, above 2^22) with five gantry angles,
+# the full 60-pair MLC and the jaws -- on a few 1e4 histories.
+def test_c1_full_geometry_bit_exact(engine, oracle):
+    job = W.config1(histories=50000)
+    assert job.meta["n"] == 60 and job.meta["voxel"] == 0.5
+    gpu, st, sh = _run(engine, job, 0, job.histories)
+    ref, _ = oracle.run(job.physics, sh, 0, job.histories)
+    _assert_same(gpu, ref)
+    assert gpu.sum() > 0
+
+
+def test_c2_full_geometry_bit_exact(engine, oracle):
+    job = W.config2(histories=30000, nphsp=30000)
+    assert sh_dims(job) == (120, 120, 120)
+    gpu, st, sh = _run(engine, job, 0, job.histories)
+    ref, _ = oracle.run(job.physics, sh, 0, job.histories)
+    _assert_same(gpu, ref)
+    assert st["processed"][5] > 0
+
+
+def test_c3_full_geometry_bit_exact(engine, oracle):
+    job = W.config3(histories=30000, nphsp=30000)
+    assert sh_dims(job) == (256, 256, 120) and len(job.fields) == 5
+    gpu, st, sh = _run(engine, job, 0, job.histories)
+    ref, _ = oracle.run(job.physics, sh, 0, job.histories)
+    _assert_same(gpu, ref)
+    assert gpu.sum() > 0
+    assert min(st["photon_steps_class"]) > 0 and min(st["electron_steps_class"]) > 0   # jaws, MLC, phantom
+
+
+def sh_dims(job):
+    p = job.phantom
+    return len(p["x_bounds"]) - 1, len(p["y_bounds"]) - 1, len(p["z_bounds"]) - 1
