@@ -31,28 +31,71 @@ def choose_options(histories, share_bytes):
     return dict(batch=b, photon_budget=32, electron_budget=8, refill_below=b // 4)
 
 
-def autotune(engine, job, sample=None, candidates=None):
-    """Time candidate settings on `sample` histories of the job; return the fastest."""
+# The autotuner's search space: each dimension's alternatives to the current
+# setting (coordinate descent from the defaults of choose_options).
+TUNE_DIMENSIONS = {
+    "batch": lambda o: [max(o["batch"] // 2, 1 << 16), min(o["batch"] * 2, 1 << 22)],
+    "blocks_per_sm": lambda o: [4, 8],
+    "photon_budget": lambda o: [16, 64],
+    "electron_budget": lambda o: [4, 16],
+    "refill_below": lambda o: [max(o["batch"] // 50, 1), max(o["batch"] // 2, 1)],
+}
+
+
+def autotune(engine, job, sample=None, candidates=None, dimensions=None, rounds=1):
+    """The fastest run options for `job`, timed on `sample` histories.
+
+    With `candidates`, each is timed and the fastest kept. Otherwise a
+    coordinate descent: starting from choose_options, each dimension of
+    TUNE_DIMENSIONS (in-flight batch, grid blocks per SM, photon and electron
+    step budgets, refill threshold) tries its alternatives with the others
+    fixed and keeps any that is faster; `rounds` passes over the dimensions.
+    Every trial first runs a quarter sample untimed (graph build, queue
+    sizing), then the timed sample; the tally is reset afterwards. Returns
+    (options, device ms of the sample, trials as a list of (options, ms))."""
     h = job.histories if sample is None else min(sample, job.histories)
-    base = choose_options(job.histories, 64e9)
-    if candidates is None:
-        b = base["batch"]
-        candidates = [dict(base), dict(base, batch=max(b // 2, 1 << 16), refill_below=max(b // 8, 1)),
-                      dict(base, photon_budget=16), dict(base, refill_below=max(b // 50, 1))]
-    best, best_t = None, float("inf")
-    for c in candidates:
-        engine.run(0, max(h // 4, 1), **c)                  # warm: builds the graph, sizes the queues
-        t = engine.run(0, h, **c)["device_ms"]
-        if t < best_t:
-            best, best_t = c, t
+    trials = []
+
+    def timed(o):
+        engine.run(0, max(h // 4, 1), **o)
+        t = engine.run(0, h, **o)["device_ms"]
+        trials.append((dict(o), t))
+        return t
+
+    if candidates is not None:
+        best, best_t = None, float("inf")
+        for c in candidates:
+            t = timed(c)
+            if t < best_t:
+                best, best_t = c, t
+        engine.reset_tally()
+        return best, best_t, trials
+    best = choose_options(job.histories, 64e9)
+    best.setdefault("blocks_per_sm", 0)
+    best_t = timed(best)
+    for _ in range(rounds):
+        for dim, alts in (dimensions or TUNE_DIMENSIONS).items():
+            for v in alts(best):
+                if v == best.get(dim):
+                    continue
+                cand = dict(best, **{dim: v})
+                if dim == "batch":
+                    cand["refill_below"] = max(v // 4, 1)
+                t = timed(cand)
+                if t < best_t:
+                    best, best_t = cand, t
     engine.reset_tally()
-    return best, best_t
+    return best, best_t, trials
 
 
 class PlanBatch:
-    def __init__(self, jobs, device=0, memory_budget_gb=40.0, tune_sample=0):
+    def __init__(self, jobs, device=0, memory_budget_gb=40.0, tune_sample=0, tune_fraction=0.0):
+        """One engine per plan. With tune_sample (histories) or tune_fraction
+        (of each plan's histories, at least 1e5), each plan's run options come
+        from the coordinate-descent autotuner, kept within the plan's share of
+        the queue-memory budget."""
         self.jobs = list(jobs)
-        self.engines, self.options = [], []
+        self.engines, self.options, self.tune_ms = [], [], []
         total = float(sum(j.histories for j in self.jobs)) or 1.0
         for job in self.jobs:
             e = Engine(device)
@@ -60,10 +103,13 @@ class PlanBatch:
             e.set_scene(job.scene())
             share = memory_budget_gb * 1e9 * job.histories / total
             opts = choose_options(job.histories, share)
-            if tune_sample:
-                opts, _ = autotune(e, job, sample=tune_sample,
-                                   candidates=[opts, dict(opts, photon_budget=16),
-                                               dict(opts, refill_below=max(opts["batch"] // 50, 1))])
+            sample = tune_sample or (int(max(1e5, tune_fraction * job.histories)) if tune_fraction > 0 else 0)
+            if sample:
+                cap = 1 << int(np.floor(np.log2(max(share / QUEUE_BYTES_PER_PARTICLE, 1 << 16))))  # what the share holds
+                dims = dict(TUNE_DIMENSIONS)
+                dims["batch"] = lambda o: [b for b in (max(o["batch"] // 2, 1 << 16), o["batch"] * 2) if b <= cap]
+                opts, t, _ = autotune(e, job, sample=sample, dimensions=dims)
+                self.tune_ms.append(t)
             self.engines.append(e)
             self.options.append(opts)
         self.wall_s = 0.0

@@ -309,7 +309,7 @@ def config5(n_plans=32, seed=SEED_BASE + 5, hist_min=1_000_000, hist_max=100_000
         h = int(np.exp(rng.uniform(np.log(hist_min), np.log(hist_max))))
         d = [int(np.exp(rng.uniform(np.log(min(dims_min, m)), np.log(m)))) for m in dims_max]
         if k % 2 == 0:
-            n = max(16, min(d))
+            n = max(dims_min, min(d))
             job = config2(histories=h, seed=seed * 100 + k, nphsp=min(nphsp, h), n=n)
             desc = f"slab {n}^3, 1 field"
         else:

@@ -15,6 +15,8 @@ import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
 LIB = HERE / "_build" / "libgegs_oracle.so"
+# -O3 -march=native build for the timed CPU baseline, made on the host that times it
+NATIVE_LIB = HERE / "_build_native" / "libgegs_oracle.so"
 
 
 class Stats(C.Structure):
@@ -30,15 +32,33 @@ def build(force=False):
     return LIB
 
 
+def build_native():
+    """The host-tuned build of the same sources (same results bit for bit)."""
+    srcs = list(HERE.glob("*.c")) + list(HERE.glob("*.h")) + list((HERE.parent / "include").glob("*.h"))
+    if not NATIVE_LIB.exists() or any(s.stat().st_mtime > NATIVE_LIB.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-s", "-C", str(HERE), "native"], check=True)
+    return NATIVE_LIB
+
+
 _lib = None
+_native = None
 
 
-def lib():
-    global _lib
+def lib(native=False):
+    global _lib, _native
+    if native:
+        if _native is None:
+            _native = _setup(C.CDLL(str(build_native())))
+        return _native
     if _lib is None:
         if not LIB.exists():
             build()
-        L = C.CDLL(str(LIB))
+        _lib = _setup(C.CDLL(str(LIB)))
+    return _lib
+
+
+def _setup(L):
+    if True:
         L.ora_log.restype = C.c_float
         L.ora_log.argtypes = [C.c_float]
         L.ora_exp.restype = C.c_float
@@ -54,8 +74,7 @@ def lib():
                               C.POINTER(C.c_int64), C.POINTER(Stats)]
         L.ora_set_trace.argtypes = [C.c_void_p, C.c_uint32]
         L.ora_trace_count.restype = C.c_uint32
-        _lib = L
-    return _lib
+    return L
 
 
 TRACE_DTYPE = np.dtype([("kind_stage", "<u4"), ("hist_lo", "<u4"), ("sid_lo", "<u4"), ("sid_hi", "<u4"),
@@ -75,9 +94,10 @@ def run_traced(physics, scene_holder, h0, h1, cap=1 << 20):
     return tally, st, buf[:min(n, cap)]
 
 
-def run(physics: np.ndarray, scene_holder, h0: int, h1: int, threads: int = 0):
-    """Run histories [h0, h1) on the CPU; returns (int64 tally, stats dict)."""
-    L = lib()
+def run(physics: np.ndarray, scene_holder, h0: int, h1: int, threads: int = 0, native: bool = False):
+    """Run histories [h0, h1) on the CPU; returns (int64 tally, stats dict).
+    native: the -O3 -march=native build (same results; for timing)."""
+    L = lib(native)
     tally = np.zeros(scene_holder.nvox, np.int64)
     st = Stats()
     phys = np.ascontiguousarray(physics)

@@ -31,3 +31,30 @@ def test_concurrent_plans_match_their_own_runs(oracle):
     ref, _ = oracle.run(jobs[1].physics, jobs[1].scene(), 0, jobs[1].histories)
     np.testing.assert_array_equal(conc[1], ref)
     pb.close()
+
+
+@pytest.mark.gpu
+def test_autotuned_plans_keep_their_tallies(oracle):
+    """The autotuner changes only how a plan runs (batch, grid, step budgets,
+    refill threshold): every candidate it times gives the same tally, and the
+    plan tuned by it still equals the oracle bit for bit."""
+    from gegs_b200.batch import PlanBatch, autotune
+    from gegs_b200.engine import Engine
+    job = W.config3(histories=6000, nphsp=4000, dims=(40, 40, 24))
+    e = Engine(0)
+    e.set_physics(job.physics)
+    e.set_scene(job.scene())
+    best, best_ms, trials = autotune(e, job, sample=3000)
+    assert len(trials) >= 8 and best_ms == min(t for _, t in trials)
+    seen = set()
+    for o, _ in trials:
+        e.reset_tally()
+        e.run(0, 3000, **o)
+        seen.add(e.tally().tobytes())
+    assert len(seen) == 1
+    e.close()
+    pb = PlanBatch([job], memory_budget_gb=2.0, tune_sample=2000)
+    pb.run()
+    ref, _ = oracle.run(job.physics, job.scene(), 0, job.histories)
+    np.testing.assert_array_equal(pb.tallies()[0], ref)
+    pb.close()
