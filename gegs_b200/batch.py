@@ -39,6 +39,7 @@ TUNE_DIMENSIONS = {
     "photon_budget": lambda o: [16, 64],
     "electron_budget": lambda o: [4, 16],
     "refill_below": lambda o: [max(o["batch"] // 50, 1), max(o["batch"] // 2, 1)],
+    "stage_tables": lambda o: [not o.get("stage_tables", False)],
 }
 
 
@@ -50,6 +51,9 @@ def autotune(engine, job, sample=None, candidates=None, dimensions=None, rounds=
     TUNE_DIMENSIONS (in-flight batch, grid blocks per SM, photon and electron
     step budgets, refill threshold) tries its alternatives with the others
     fixed and keeps any that is faster; `rounds` passes over the dimensions.
+    Dimensions: in-flight batch, grid blocks per SM, photon and electron step
+    budgets, refill threshold, and whether the photon tables are staged in
+    shared memory (GEGS_RUN_STAGE_TABLES).
     Every trial first runs a quarter sample untimed (graph build, queue
     sizing), then the timed sample; the tally is reset afterwards. Returns
     (options, device ms of the sample, trials as a list of (options, ms))."""

@@ -18,6 +18,7 @@
 #include <cooperative_groups.h>
 #include "../../include/gegs_physics.h"
 #include "../../include/gegs_scene.h"
+#include "gx_cmp.h"
 
 namespace cg = cooperative_groups;
 
@@ -158,6 +159,13 @@ __device__ __forceinline__ uint32_t fastdiv(const FastDiv &f, uint32_t n)
 // Everything a transport kernel needs; passed by value as a kernel parameter.
 struct DevCtx {
     const gegs_physics *P;
+    // Tables re-laid out on the device from P (same values, read together):
+    //   ptab[med*MXGE + lgle] = {gmfp.a, gmfp.b, cohe.a, cohe.b}: the photon mean
+    //     free path and Rayleigh factor of one step, the slice the photon
+    //     consumers stage in shared memory when stage_tables is set.
+    const float4 *ptab;
+    int nmed;
+    uint32_t stage_tables;          // GEGS_RUN_STAGE_TABLES of the run
     const Vox *reg;                 // nvox + 6 regions
     const float *xb, *yb, *zb;
     const gegs_field *fields;

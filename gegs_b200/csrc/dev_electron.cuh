@@ -14,7 +14,7 @@ __device__ __forceinline__ float ev2(float2 t, float x) { return t.x + t.y * x; 
 __device__ void mscat(const DevCtx &C, float lambda, float chia2, float q1, float &cost, float &sint, Rng &r)
 {
     const gegs_physics *P = C.P;
-    if (lambda <= 13.8) {
+    if (gx_le(lambda, 13.8)) {
         float sprob = U(C, r);
         float explambda = gx_exp(-lambda);
         if (sprob < explambda) { cost = 1.0f; sint = 0.0f; return; }
@@ -41,7 +41,7 @@ __device__ void mscat(const DevCtx &C, float lambda, float chia2, float q1, floa
                 xi = 2.0f * chia2 * xi / (1.0f - xi + chia2);
                 float cosz = 1.0f - xi;
                 float sinz = xi * (2.0f - xi);
-                if (sinz > 1.0e-20) {
+                if (gx_gt(sinz, 1.0e-20)) {
                     sinz = sqrtf(sinz);
                     xi = U(C, r);
                     float phi = xi * 6.2831853;
@@ -57,7 +57,7 @@ __device__ void mscat(const DevCtx &C, float lambda, float chia2, float q1, floa
             return;
         }
     }
-    if (lambda <= 1e5) {
+    if (gx_le(lambda, 1e5)) {
         float llmbda = gx_log(lambda);
         float ai = llmbda * P->dllambi;
         int msi = (int)ai;
@@ -66,7 +66,7 @@ __device__ void mscat(const DevCtx &C, float lambda, float chia2, float q1, floa
         if (xi < ai) msi = msi + 1;
         if (msi > GEGS_MAXL_MS) msi = GEGS_MAXL_MS;
         int msj;
-        if (q1 < 1e-3) msj = 0;
+        if (gx_lt(q1, 1e-3)) msj = 0;
         else if (q1 < 0.5f) {
             float aj = q1 * P->dqmsi;
             msj = (int)aj;
@@ -75,7 +75,7 @@ __device__ void mscat(const DevCtx &C, float lambda, float chia2, float q1, floa
             if (xi < aj) msj = msj + 1;
         } else msj = GEGS_MAXQ_MS;
         float omega2;
-        if (llmbda < 2.2299)
+        if (gx_lt(llmbda, 2.2299))
             omega2 = chia2 * (lambda + 4) * (1.347006 + llmbda * (0.209364 - llmbda * (0.45525 - llmbda * (0.50142 - 0.081234 * llmbda))));
         else
             omega2 = chia2 * (lambda + 4) * (-2.77164 + llmbda * (2.94874 - llmbda * (0.1535754 - llmbda * 0.00552888)));
@@ -94,13 +94,13 @@ __device__ void mscat(const DevCtx &C, float lambda, float chia2, float q1, floa
         float u = __ldg(&P->ums_array[idx]);
         float du = __ldg(&P->ums_array[((msk + 1) * sj + msj) * sl + msi]) - u;
         xi = U(C, r);
-        if (fabsf(a) < 0.2) {
+        if (gx_lt(fabsf(a), 0.2)) {
             float x1 = 0.5 * (1 - xi) * a;
             u = u + xi * du * (1.0f + x1 * (1.0f - xi * a));
         } else
             u = u - du / a * (1.0f - sqrtf(1.0f + xi * a * (2.0f + a)));
         xi = omega2 * u / (1 + 0.5 * omega2 - u);
-        if (xi > 1.99999) xi = 1.99999;
+        if (gx_gt(xi, 1.99999)) xi = (float)1.99999;
         cost = 1.0f - xi;
         sint = sqrtf(xi * (2.0f - xi));
         return;
@@ -145,7 +145,7 @@ __device__ void msdist_pI(const DevCtx &C, float eloss, float tustep, Part &p0, 
     float us = sint * cphi;
     float vs = sint * sphi;
     float z, rr, r2, z2, r2max;
-    if (xi < 0.1) z = 1 - xi * (0.5 - xi * (0.166666667 - 0.041666667 * xi));
+    if (gx_lt(xi, 0.1)) z = 1 - xi * (0.5 - xi * (0.166666667 - 0.041666667 * xi));
     else z = (1.0f - gx_exp(-xi)) / xi;
     rr = 0.5 * sint;
     r2 = rr * rr;
@@ -155,7 +155,7 @@ __device__ void msdist_pI(const DevCtx &C, float eloss, float tustep, Part &p0, 
     float ut = rr * cphi, vt = rr * sphi, wt = z;
     ustep = sqrtf(z2 + r2) * tustep;
     float sint02 = p0.u * p0.u + p0.v * p0.v;
-    if (sint02 > 1e-20) {
+    if (gx_gt(sint02, 1e-20)) {
         float sint0 = sqrtf(sint02);
         float cphi0 = p0.u / sint0;
         float sphi0 = p0.v / sint0;
@@ -393,7 +393,7 @@ __device__ int electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
                 chia2 = xccl / (4.0f * blccl * p2);
                 xi = 0.5 * xccl / p2 / beta2 * tustep;
                 xi = xi * (gx_log((float)(1 + 1.0 / chia2)) - 1 / (1 + chia2));
-                if (xi < 0.1) ustep = tustep * (1 - xi * (0.5 - xi * 0.166667));
+                if (gx_lt(xi, 0.1)) ustep = tustep * (1 - xi * (0.5 - xi * 0.166667));
                 else ustep = tustep * (1.0f - gx_exp(-xi)) / xi;
             }
             callhowfar = !(ustep < tperp);
@@ -448,9 +448,9 @@ __device__ int electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
                 chia2 = xccl / (4.0f * blccl * p2);
                 xi = 0.5 * xccl / p2 / beta2 * vstep;
                 xi = xi * (gx_log((float)(1 + 1.0 / chia2)) - 1 / (1 + chia2));
-                if (xi < 0.1) tvstep = vstep * (1 + xi * (0.5 + xi * 0.333333));
+                if (gx_lt(xi, 0.1)) tvstep = vstep * (1 + xi * (0.5 + xi * 0.333333));
                 else {
-                    if (xi < 0.999999) tvstep = -vstep * gx_log(1 - xi) / xi;
+                    if (gx_lt(xi, 0.999999)) tvstep = -vstep * gx_log(1 - xi) / xi;
                     else return true;
                 }
             } else tvstep = tustep;
@@ -509,8 +509,8 @@ __device__ int electron_step(const DevCtx &C, Part &p, Rng &r, EState &s)
     if (medium != medold) { s.is_tstep = true; return false; }
     s.demfp = s.demfp - save_de * sig_val;
     s.total_tstep = s.total_tstep - tvstep * rhof;
-    if (s.total_tstep < 1e-9) s.demfp = 0.0f;
-    if (s.demfp >= GX_EPSEMFP) { s.is_tstep = false; return false; }
+    if (gx_lt(s.total_tstep, 1e-9)) s.demfp = 0.0f;
+    if (gx_ge(s.demfp, GX_EPSEMFP)) { s.is_tstep = false; return false; }
     float sigf = ev2(tab2(P->sig, qel * GX_MXEKE * GX_MXMED + medium * GX_MXEKE + s.lelke - 1), s.elke);
     float dedx0 = ev2(tab2(P->dedx, qel * GX_MXEKE * GX_MXMED + medium * GX_MXEKE + s.lelke - 1), s.elke);
     sigf = sigf / dedx0;
@@ -703,7 +703,7 @@ __device__ void brems(const DevCtx &C, Part p, Rng &r)
     int nbr = P->nbr_split;
     if (nbr < 1) return;
     float eie = p.e;
-    int l = (eie < 50.0) ? 1 : 3;
+    int l = gx_lt(eie, 50.0) ? 1 : 3;
     int l1 = l + 1;
     float ekin = eie - prm;
     float elke = gx_log(ekin);
@@ -715,7 +715,7 @@ __device__ void brems(const DevCtx &C, Part p, Rng &r)
     if (ibrdst >= 0) {
         a = p.u; b = p.v; c = p.w;
         sinpsi = a * a + b * b;
-        if (sinpsi > 1e-20) {
+        if (gx_gt(sinpsi, 1e-20)) {
             sinpsi = sqrtf(sinpsi);
             sindel = b / sinpsi;
             cosdel = a / sinpsi;
@@ -791,7 +791,7 @@ __device__ void brems(const DevCtx &C, Part p, Rng &r)
             float sinthe = sqrtf(fmaxf_((1.0f - costhe) * (1.0f + costhe), 0.0f));
             float cphi, sphi;
             box_phi(C, r, cphi, sphi);
-            if (sinpsi >= 1e-10) {
+            if (gx_ge(sinpsi, 1e-10)) {
                 float us = sinthe * cphi;
                 float vs = sinthe * sphi;
                 p1.u = c * cosdel * us - sindel * vs + a * costhe;
@@ -891,7 +891,7 @@ __device__ void annih(const DevCtx &C, Part p, Rng &r)
     float wsamp = gx_log((1.0f - ep0) / ep0);
     float aa = p.u, bb = p.v, cc = p.w;
     float sinpsi = aa * aa + bb * bb, sindel = 0.0f, cosdel = 0.0f;
-    if (sinpsi > 1e-20) {
+    if (gx_gt(sinpsi, 1e-20)) {
         sinpsi = sqrtf(sinpsi);
         sindel = bb / sinpsi;
         cosdel = aa / sinpsi;
@@ -913,7 +913,7 @@ __device__ void annih(const DevCtx &C, Part p, Rng &r)
         float sinthe = sqrtf(1.0f - costhe * costhe);
         float cphi, sphi;
         box_phi(C, r, cphi, sphi);
-        if (sinpsi >= 1e-10) {
+        if (gx_ge(sinpsi, 1e-10)) {
             float us = sinthe * cphi, vs = sinthe * sphi;
             p.u = cc * cosdel * us - sindel * vs + aa * costhe;
             p.v = cc * sindel * us + cosdel * vs + bb * costhe;
@@ -927,7 +927,7 @@ __device__ void annih(const DevCtx &C, Part p, Rng &r)
         p.e = esg2;
         costhe = fminf_(1.0f, (esg2 - rm) * pot / esg2);
         sinthe = -sqrtf(1.0f - costhe * costhe);
-        if (sinpsi >= 1e-10) {
+        if (gx_ge(sinpsi, 1e-10)) {
             float us = sinthe * cphi, vs = sinthe * sphi;
             p.u = cc * cosdel * us - sindel * vs + aa * costhe;
             p.v = cc * sindel * us + cosdel * vs + bb * costhe;

@@ -174,9 +174,30 @@ __device__ void relax(const DevCtx &C, float energy, int n, int iz, float &edep,
     }
 }
 
+// With C.stage_tables (run option GEGS_RUN_STAGE_TABLES) the photon consumers
+// stage the {gmfp, cohe} table of the plan's media (C.ptab, nmed * MXGE
+// float4, 19.2 KB for six media) in dynamic shared memory once per block, and
+// a step reads its mean free path and Rayleigh factor from there; otherwise
+// from the physics block through L1/L2. Same values either way. On the CT
+// 5-field plan the staged form is 1.2 % slower (the slice is L1-resident and
+// the carve-out shrinks L1 for the region gathers), so it is an option the
+// batch autotuner can pick per plan.
+extern __shared__ float4 g_smem_ptab[];
+
+__host__ __device__ constexpr size_t photon_smem_bytes(int nmed) { return (size_t)nmed * GX_MXGE * sizeof(float4); }
+
+__device__ __forceinline__ void stage_photon_tables(const DevCtx &C)
+{
+    if (!C.stage_tables) return;
+    const int n = C.nmed * GX_MXGE;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) g_smem_ptab[i] = __ldg(&C.ptab[i]);
+    __syncthreads();
+}
+
 // One iteration of the PHOTON loop.  Returns true when the photon has left
 // the photon stage (absorbed, escaped or queued for an interaction).
-template <int G = GX_GEOM_ALL>
+// SH: the {gmfp, cohe} table is staged in shared memory (stage_photon_tables).
+template <int G = GX_GEOM_ALL, bool SH = false>
 __device__ bool photon_step(const DevCtx &C, Part &p, Rng &r)
 {
     const gegs_physics *P = C.P;
@@ -193,12 +214,20 @@ __device__ bool photon_step(const DevCtx &C, Part &p, Rng &r)
     else {
         float2 ge = __ldg(reinterpret_cast<const float2 *>(P->ge[med]));
         lgle = (int)(ge.x + ge.y * gle);
-        float2 g = __ldg(reinterpret_cast<const float2 *>(P->gmfp[med * GX_MXGE + lgle]));
-        float gmfpr0 = g.x + g.y * gle;
+        float4 t;
+        if (SH && C.stage_tables) t = g_smem_ptab[med * GX_MXGE + lgle];
+        else {
+            const float2 g = __ldg(reinterpret_cast<const float2 *>(P->gmfp[med * GX_MXGE + lgle]));
+            t.x = g.x; t.y = g.y;
+        }
+        float gmfpr0 = t.x + t.y * gle;
         gmfp_val = gmfpr0 / rd.rhof;
         if (rd.flags & GEGS_F_RAYLEIGH) {
-            float2 c = __ldg(reinterpret_cast<const float2 *>(P->cohe[med * GX_MXGE + lgle]));
-            cohfac = c.x + c.y * gle;
+            if (!(SH && C.stage_tables)) {
+                const float2 c = __ldg(reinterpret_cast<const float2 *>(P->cohe[med * GX_MXGE + lgle]));
+                t.z = c.x; t.w = c.y;
+            }
+            cohfac = t.z + t.w * gle;
             gmfp_val = gmfp_val * cohfac;
         }
         tstep = gmfp_val * dpmfp;
@@ -218,7 +247,7 @@ __device__ bool photon_step(const DevCtx &C, Part &p, Rng &r)
     unsigned old_medium = med;
     if (new_region != p.region) { p.region = new_region; rd = region_info(C, new_region); }
     if (p.e <= rd.pcut || idisc < 0) { escore(C, p, p.region, p.e * p.wt); return true; }
-    if ((rd.med != old_medium) || (rd.med == GX_VACUUM) || (dpmfp >= GX_EPSGMFP)) return false;
+    if ((rd.med != old_medium) || (rd.med == GX_VACUUM) || gx_ge(dpmfp, GX_EPSGMFP)) return false;
     if (rd.flags & GEGS_F_RAYLEIGH) {
         r1 = U(C, r);
         if (r1 < 1.0f - cohfac) { push_move(C, ST_RAYLEIGH, p, r); return true; }
@@ -340,8 +369,8 @@ __device__ void compton(const DevCtx &C, Part p, Rng &r)
                     af = 0.0f; fmax1 = 1.0f;
                 } else {
                     float fpz1;
-                    if (pzmax < -0.15) { fmax1 = 1 - af * 0.15; fpz1 = fpz * fmax1 * jo; }
-                    else if (pzmax < 0.15) {
+                    if (gx_lt(pzmax, -0.15)) { fmax1 = 1 - af * 0.15; fpz1 = fpz * fmax1 * jo; }
+                    else if (gx_lt(pzmax, 0.15)) {
                         fmax1 = 1.0f + af * pzmax;
                         aux3 = 1 / (1 + 0.33267252734 * aux3);
                         aux4 = fpz * aux3 * (0.3480242 + aux3 * (-0.0958798 + aux3 * 0.7478556)) + __ldg(&P->erfjo_array[j - 1]);
@@ -369,21 +398,21 @@ __device__ void compton(const DevCtx &C, Part p, Rng &r)
                         pz = 0.5 * (sqrtf(1 - 2 * gx_log(rnno18)) - 1) / jo;
                     }
                     if (fabsf(pz) > 1.0f) continue;
-                    if (pz < 0.15) {
+                    if (gx_lt(pz, 0.15)) {
                         float frej;
-                        if (pz < -0.15) frej = 1 - af * 0.15; else frej = 1.0f + af * pz;
+                        if (gx_lt(pz, -0.15)) frej = 1 - af * 0.15; else frej = 1.0f + af * pz;
                         float eta = U(C, r);
                         if (eta * fmax1 > frej) continue;
                     }
                 } else { pz = 0.0f; uj = 0.0f; }
                 break;
             }
-            if (fabsf(pz) < 0.01) br = br * (1.0f + pz * (qc + (br * br - costhe) * pz));
+            if (gx_lt(fabsf(pz), 0.01)) br = br * (1.0f + pz * (qc + (br * br - costhe) * pz));
             else {
                 float a1 = 1.0f - pz * pz * br * costhe;
                 float a2 = 1.0f - pz * pz * br * br;
                 float a3 = qc2 - br * br * pz * pz * sinthe;
-                if (a3 > 1e-10) br = br / a2 * (a1 + pz * sqrtf(a3));
+                if (gx_gt(a3, 1e-10)) br = br / a2 * (a1 + pz * sqrtf(a3));
             }
             uj = uj * prm;
         }
@@ -396,7 +425,7 @@ __device__ void compton(const DevCtx &C, Part p, Rng &r)
         if (p.e < rd.pcut) edep += p.e;
         else push_spawn(C, ST_PHOTON, p, r);
         float aux = 1.0f + br * br - 2.0f * br * costhe;
-        if (aux > 1e-8) {
+        if (gx_gt(aux, 1e-8)) {
             costhe = (1.0f - br * costhe) / sqrtf(aux);
             sinthe = (1.0f - costhe) * (1.0f + costhe);
             if (sinthe > 0.0f) sinthe = -sqrtf(sinthe); else sinthe = 0.0f;
@@ -407,7 +436,7 @@ __device__ void compton(const DevCtx &C, Part p, Rng &r)
         if (p1.e < rd.ecut) edep += p1.e - prm;
         else push_spawn(C, ST_ELECTRON, p1, r);
         if ((ibcmpl == 1) || (ibcmpl == 3)) {
-            if (uj > 0.001)
+            if (gx_gt(uj, 0.001))
                 relax(C, uj, __ldg(&P->shn_array[j - 1]), __ldg(&P->iz_array[j - 1]), edep, p, rd, r);
             else edep += uj;
         }
@@ -511,7 +540,7 @@ __device__ void photo(const DevCtx &C, Part p, Rng &r)
                 do {
                     float rnpht = U(C, r);
                     rnpht = 2.0f * rnpht - 1.0f;
-                    if (ratio <= 0.2) {
+                    if (gx_le(ratio, 0.2)) {
                         float fkappa = rnpht + 0.5 * ratio * (1.0f - rnpht) * (1 + rnpht);
                         if (gamma < 100.0f) costhe = (beta + fkappa) / (1.0f + beta * fkappa);
                         else {
@@ -683,7 +712,7 @@ __device__ void pair(const DevCtx &C, Part p, Rng &r)
     float eig = p.e;
     float ese1, ese2;
     int iq1, iq2;
-    if (eig <= 2.1) {
+    if (gx_le(eig, 2.1)) {
         float rnno30 = U(C, r);
         ese2 = prm + 0.5 * rnno30 * (eig - 2 * prm);
         rnno30 = U(C, r);
@@ -757,7 +786,7 @@ __device__ void pair(const DevCtx &C, Part p, Rng &r)
             float rtest = U(C, r);
             float gbeta = ese1 / (ese1 + 10.0f);
             use = (rtest < gbeta) ? 1 : 4;
-        } else if ((iprdst == 2) && (eig < 4.14)) use = 1;
+        } else if ((iprdst == 2) && gx_lt(eig, 4.14)) use = 1;
         else use = iprdst;
         for (int ichrg = 1; ichrg <= 2; ichrg++) {
             float ese;

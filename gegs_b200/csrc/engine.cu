@@ -47,6 +47,7 @@ struct gegs_engine {
     std::string err;
 
     gegs_physics *d_P = nullptr;
+    float4 *d_ptab = nullptr;          // {gmfp, cohe} per (medium, energy bin) (DevCtx::ptab)
     Vox *d_reg = nullptr;
     float *d_xb = nullptr, *d_yb = nullptr, *d_zb = nullptr;
     gegs_field *d_fields = nullptr;
@@ -195,7 +196,7 @@ void gegs_destroy(gegs_engine *e)
     if (e->stream) cudaStreamSynchronize(e->stream);
     for (int k = 0; k < 2; k++) if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
     cudaFree(e->d_blw); cudaFree(e->d_gvm); cudaFree(e->d_grad);
-    cudaFree(e->d_P); cudaFree(e->d_reg); cudaFree(e->d_xb); cudaFree(e->d_yb); cudaFree(e->d_zb);
+    cudaFree(e->d_P); cudaFree(e->d_ptab); cudaFree(e->d_reg); cudaFree(e->d_xb); cudaFree(e->d_yb); cudaFree(e->d_zb);
     cudaFree(e->d_timeline);
     cudaFree(e->d_fields); cudaFree(e->d_cross); cudaFree(e->d_jaw_lines); cudaFree(e->d_phsp); cudaFree(e->d_tally);
     cudaFree(e->d_err); cudaFree(e->d_stats); cudaFree(e->d_sched); cudaFree(e->d_qmeta);
@@ -237,6 +238,9 @@ gegs_status gegs_check_physics(const gegs_physics *P, char *msg, size_t msg_len)
 #undef GX_CHECK_FINITE
     for (int m = 0; m < P->nmed; m++)
         if (!(P->rho[m] > 0.0f)) return fail("physics block: a medium has a density that is not positive");
+    for (int i = 0; i < GEGS_MS_SIZE; i++)        // alias bins of the scattering tables (the sampler reads bin + 1)
+        if (P->ims_array[i] < 0 || P->ims_array[i] > GEGS_MAXU_MS - 1)
+            return fail("physics block: ims_array holds a bin outside 0..GEGS_MAXU_MS-1");
     if (msg && msg_len) msg[0] = '\0';
     return GEGS_OK;
 }
@@ -251,9 +255,18 @@ gegs_status gegs_set_physics(gegs_engine *e, const gegs_physics *P)
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     if (!e->d_P) CK(cudaMalloc(&e->d_P, sizeof(gegs_physics)), "physics");
     CK(cudaMemcpyAsync(e->d_P, P, sizeof(gegs_physics), cudaMemcpyHostToDevice, e->stream), "physics H2D");
+    // {gmfp, cohe} interleaved, the slice a photon step reads (see DevCtx::ptab)
+    const size_t ng = (size_t)GEGS_MXMED * GEGS_MXGE;
+    std::vector<float4> ptab(ng);
+    for (size_t i = 0; i < ng; i++)
+        ptab[i] = make_float4(P->gmfp[i][0], P->gmfp[i][1], P->cohe[i][0], P->cohe[i][1]);
+    if (!e->d_ptab) CK(cudaMalloc(&e->d_ptab, ng * sizeof(float4)), "photon tables");
+    CK(cudaMemcpyAsync(e->d_ptab, ptab.data(), ng * sizeof(float4), cudaMemcpyHostToDevice, e->stream), "tables H2D");
     CK(cudaStreamSynchronize(e->stream), "physics sync");
     e->have_physics = true;
     e->ctx.P = e->d_P;
+    e->ctx.ptab = e->d_ptab;
+    e->ctx.nmed = P->nmed;
     e->ctx_gen++;
     return GEGS_OK;
 }
@@ -471,9 +484,10 @@ static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
     };
     k_source<<<grid, threads, 0, s>>>(C, e->d_sched);
     fork(2);
-    k_photon_jaws<<<grid, threads, 0, a[0]>>>(C);
-    k_photon_mlc<<<grid, threads, 0, a[1]>>>(C);
-    k_photon<<<grid, threads, 0, s>>>(C);
+    const size_t ps = C.stage_tables ? photon_smem_bytes(C.nmed) : 0;   // the staged {gmfp, cohe} table
+    k_photon_jaws<<<grid, threads, ps, a[0]>>>(C);
+    k_photon_mlc<<<grid, threads, ps, a[1]>>>(C);
+    k_photon<<<grid, threads, ps, s>>>(C);
     join(2);
     fork(3);
     k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(C);
@@ -482,7 +496,7 @@ static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
     k_interact<ST_PAIR><<<grid, threads, 0, a[2]>>>(C);
     join(3);
     fork(3);
-    k_photon_jaws_long<<<grid, threads, 0, a[2]>>>(C);
+    k_photon_jaws_long<<<grid, threads, ps, a[2]>>>(C);
     k_electron_jaws<<<grid, threads, 0, a[0]>>>(C);
     k_electron_jaws_near<<<grid, threads, 0, a[0]>>>(C);
     k_electron_mlc<<<grid, threads, 0, a[1]>>>(C);
@@ -547,6 +561,8 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
     int bps = o.blocks_per_sm ? o.blocks_per_sm : 6;
     int grid = e->nsm * bps;
     uint32_t max_waves = o.max_waves ? o.max_waves : 200000u;
+    const uint32_t stage = (o.flags & GEGS_RUN_STAGE_TABLES) ? 1u : 0u;
+    if (stage != e->ctx.stage_tables) { e->ctx.stage_tables = stage; e->ctx_gen++; }
     uint32_t pb = (o.step_budget & 0xFFFFu) ? (o.step_budget & 0xFFFFu) : 32u;
     uint32_t eb = (o.step_budget >> 16) ? (o.step_budget >> 16) : 4u;
     if (pb != e->ctx.photon_budget || eb != e->ctx.electron_budget) {
@@ -616,17 +632,17 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
                 CK(cudaEventRecord(evs[2 * k], s), "event");
                 switch (slot[k]) {
                 case 10: k_source<<<grid, threads, 0, s>>>(C, e->d_sched); break;
-                case 12: k_photon_jaws<<<grid, threads, 0, s>>>(C); break;
+                case 12: k_photon_jaws<<<grid, threads, C.stage_tables ? photon_smem_bytes(C.nmed) : 0, s>>>(C); break;
                 case 13:
                     k_electron_jaws<<<grid, threads, 0, s>>>(C);
                     k_electron_jaws_near<<<grid, threads, 0, s>>>(C);
                     break;
-                case 14: k_photon_mlc<<<grid, threads, 0, s>>>(C); break;
+                case 14: k_photon_mlc<<<grid, threads, C.stage_tables ? photon_smem_bytes(C.nmed) : 0, s>>>(C); break;
                 case 15:
                     k_electron_mlc<<<grid, threads, 0, s>>>(C);
                     k_electron_mlc_near<<<grid, threads, 0, s>>>(C);
                     break;
-                case ST_PHOTON: k_photon<<<grid, threads, 0, s>>>(C); break;
+                case ST_PHOTON: k_photon<<<grid, threads, C.stage_tables ? photon_smem_bytes(C.nmed) : 0, s>>>(C); break;
                 case ST_COMPTON: k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(C); break;
                 case ST_PHOTO: k_interact<ST_PHOTO><<<grid, threads, 0, s>>>(C); break;
                 case ST_RAYLEIGH: k_interact<ST_RAYLEIGH><<<grid, threads, 0, s>>>(C); break;
@@ -1006,6 +1022,7 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
     c.trace = nullptr;
     c.trace_n = nullptr;
     c.trace_cap = 0;
+    c.stage_tables = 0u;
     c.photon_budget = 16u;
     c.electron_budget = 8u;
 

@@ -264,6 +264,7 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     constexpr bool LONG = !ELEC && G == GX_GEOM_JAWS && NEAR;
     constexpr int tl = LONG ? TL_PLONG : NEAR ? TL_ENEAR : (ELEC ? TL_ELECTRON : TL_PHOTON) + cls;
     timeline_mark(C, tl, false);
+    if (!ELEC) stage_photon_tables(C);
     const uint32_t par = *C.wave & 1u;
     const int qc_in = LONG ? GX_Q_PLONG : NEAR ? GX_Q_ENEAR + cls : base + 2 * cls + (int)par;
     const int qc_out = base + 2 * cls + (int)(par ^ 1u);
@@ -323,7 +324,7 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
                         steps--;
                     }
                     done = code != 0;                 // leaves this pass either way
-                } else done = ELEC ? electron_step<G>(C, p, r, s) != 0 : photon_step<G>(C, p, r);
+                } else done = ELEC ? electron_step<G>(C, p, r, s) != 0 : photon_step<G, true>(C, p, r);
                 if (done) active = false;
                 else if (++nst >= budget &&
                          (!JAWS_PHOTON || !C.overlap || nst >= 64u * budget ||

@@ -37,7 +37,9 @@ class GegsError(RuntimeError):
 class RunOpts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("batch", C.c_uint32), ("blocks_per_sm", C.c_int32),
                 ("threads_per_block", C.c_int32), ("max_waves", C.c_uint32), ("step_budget", C.c_uint32),
-                ("refill_below", C.c_uint32), ("queue_cap", C.c_uint32)]
+                ("refill_below", C.c_uint32), ("queue_cap", C.c_uint32), ("flags", C.c_uint32)]
+
+RUN_STAGE_TABLES = 1
 
 
 class RunStats(C.Structure):
@@ -156,7 +158,7 @@ class Engine:
         if g.size != self.nvox:
             raise ValueError(f"voxel gradient has {g.size} entries for {self.nvox} voxels")
         out = np.zeros(self.nbeamlets, np.float64)
-        o = RunOpts(MODE_PERSISTENT, batch, 0, 0, 0, 0, 0, 0)
+        o = RunOpts(MODE_PERSISTENT, batch, 0, 0, 0, 0, 0, 0, 0)
         self._check(self.L.gegs_backward(self.h, h0, h1, g.ctypes.data, out.ctypes.data, out.size, C.byref(o)))
         return out
 
@@ -166,17 +168,17 @@ class Engine:
 
     def run(self, h0: int, h1: int, mode: int = MODE_PERSISTENT, batch: int = 0, blocks_per_sm: int = 0,
             threads: int = 0, max_waves: int = 0, photon_budget: int = 0, electron_budget: int = 0,
-            refill_below: int = 0, queue_cap: int = 0):
+            refill_below: int = 0, queue_cap: int = 0, stage_tables: bool = False):
         o = RunOpts(mode, batch, blocks_per_sm, threads, max_waves, (photon_budget & 0xFFFF) | (electron_budget << 16),
-                    refill_below, queue_cap)
+                    refill_below, queue_cap, RUN_STAGE_TABLES if stage_tables else 0)
         self._check(self.L.gegs_run(self.h, h0, h1, C.byref(o)))
         return self.stats()
 
     def launch(self, h0: int, h1: int, batch: int = 0, blocks_per_sm: int = 0, threads: int = 0,
-               photon_budget: int = 0, electron_budget: int = 0, refill_below: int = 0):
+               photon_budget: int = 0, electron_budget: int = 0, refill_below: int = 0, stage_tables: bool = False):
         """Queue a persistent-form run and return at once (see wait())."""
         o = RunOpts(MODE_PERSISTENT, batch, blocks_per_sm, threads, 0, (photon_budget & 0xFFFF) | (electron_budget << 16),
-                    refill_below, 0)
+                    refill_below, 0, RUN_STAGE_TABLES if stage_tables else 0)
         self._check(self.L.gegs_launch(self.h, h0, h1, C.byref(o)))
 
     def wait(self):

@@ -69,7 +69,12 @@ typedef struct gegs_run_opts {
                                   `batch`). A queue that would overflow drops nothing silently: the run
                                   stops after the wave and returns GEGS_ERR_QUEUE_FULL (the reference
                                   drops the particle with a message, utility.cu:270-275) */
+    uint32_t flags;            /* GEGS_RUN_STAGE_TABLES: photon consumers stage the mean-free-path and
+                                  Rayleigh tables of the plan's media in shared memory (same results;
+                                  1.2 % slower on the CT 5-field plan, an autotuner choice per plan) */
 } gegs_run_opts;
+
+#define GEGS_RUN_STAGE_TABLES 1u
 
 typedef struct gegs_run_stats {
     uint64_t processed[10];    /* particles handled per stage: photon, compton, photo, rayleigh,

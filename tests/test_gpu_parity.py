@@ -153,3 +153,15 @@ def test_c3_full_geometry_bit_exact(engine, oracle):
 def sh_dims(job):
     p = job.phantom
     return len(p["x_bounds"]) - 1, len(p["y_bounds"]) - 1, len(p["z_bounds"]) - 1
+
+
+def test_tables_staged_in_shared_memory_bit_exact(engine, oracle):
+    """GEGS_RUN_STAGE_TABLES: the photon consumers read the mean-free-path and
+    Rayleigh tables from shared memory; the tally is the oracle's, as without."""
+    job = W.config3(histories=8000, nphsp=6000, dims=(48, 48, 24))
+    gpu, st, sh = _run(engine, job, 0, job.histories, stage_tables=True)
+    ref, _ = oracle.run(job.physics, sh, 0, job.histories)
+    _assert_same(gpu, ref)
+    engine.reset_tally()
+    engine.run(0, job.histories, mode=2, stage_tables=True)          # the timed form launches them by name
+    _assert_same(engine.tally(), ref)
