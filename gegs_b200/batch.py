@@ -43,7 +43,7 @@ TUNE_DIMENSIONS = {
 }
 
 
-def autotune(engine, job, sample=None, candidates=None, dimensions=None, rounds=1):
+def autotune(engine, job, sample=None, candidates=None, dimensions=None, rounds=1, start=None):
     """The fastest run options for `job`, timed on `sample` histories.
 
     With `candidates`, each is timed and the fastest kept. Otherwise a
@@ -55,7 +55,8 @@ def autotune(engine, job, sample=None, candidates=None, dimensions=None, rounds=
     budgets, refill threshold, and whether the photon tables are staged in
     shared memory (GEGS_RUN_STAGE_TABLES).
     Every trial first runs a quarter sample untimed (graph build, queue
-    sizing), then the timed sample; the tally is reset afterwards. Returns
+    sizing), then the timed sample; the tally is reset afterwards. `start`
+    replaces choose_options' defaults (a batch within a memory share). Returns
     (options, device ms of the sample, trials as a list of (options, ms))."""
     h = job.histories if sample is None else min(sample, job.histories)
     trials = []
@@ -74,7 +75,7 @@ def autotune(engine, job, sample=None, candidates=None, dimensions=None, rounds=
                 best, best_t = c, t
         engine.reset_tally()
         return best, best_t, trials
-    best = choose_options(job.histories, 64e9)
+    best = dict(start) if start is not None else choose_options(job.histories, 64e9)
     best.setdefault("blocks_per_sm", 0)
     best_t = timed(best)
     for _ in range(rounds):
@@ -112,7 +113,7 @@ class PlanBatch:
                 cap = 1 << int(np.floor(np.log2(max(share / QUEUE_BYTES_PER_PARTICLE, 1 << 16))))  # what the share holds
                 dims = dict(TUNE_DIMENSIONS)
                 dims["batch"] = lambda o: [b for b in (max(o["batch"] // 2, 1 << 16), o["batch"] * 2) if b <= cap]
-                opts, t, _ = autotune(e, job, sample=sample, dimensions=dims)
+                opts, t, _ = autotune(e, job, sample=sample, dimensions=dims, start=opts)
                 self.tune_ms.append(t)
             self.engines.append(e)
             self.options.append(opts)
