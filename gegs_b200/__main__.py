@@ -142,7 +142,16 @@ def main(argv=None):
     ap.add_argument("--uncertainty", type=int, default=0, metavar="BATCHES",
                     help="also write the relative standard error per voxel from this many batches "
                          "(the reference's GET_UNCERTAINTY output)")
+    ap.add_argument("--write-physics", metavar="FILE", default=None,
+                    help="write the plan's physics tables for C/C++ callers (gegs_plan_load) and exit")
     a = ap.parse_args(argv)
+    if a.write_physics:
+        from . import physics_data as PD
+        from .plan import load_plan
+        plan = load_plan(a.input, max_histories=a.max_histories)
+        PD.write_physics_file(a.write_physics, plan.job.media, plan.job.physics)
+        print(f"physics for media {plan.job.media} written to {a.write_physics}")
+        return
     run_plan(a.input, a.device, a.max_histories, uncertainty_batches=a.uncertainty)
 
 

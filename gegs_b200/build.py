@@ -24,7 +24,8 @@ NVCC_FLAGS = [
 
 
 def sources():
-    return sorted(list(SRC.glob("*.cu")) + list(SRC.glob("*.cuh")) + list(INC.glob("*.h")))
+    return sorted(list(SRC.glob("*.cu")) + list(SRC.glob("*.cuh")) + list(SRC.glob("*.cpp")) + list(SRC.glob("*.h"))
+                  + list(INC.glob("*.h")))
 
 
 def needs_build() -> bool:
@@ -38,7 +39,8 @@ def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
     if not force and not needs_build():
         return LIB
     nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, "-o", str(LIB), str(SRC / "engine.cu"), str(SRC / "postproc.cu")]
+    cmd = [nvcc, *NVCC_FLAGS, "-Xcompiler", "-ffp-contract=off", "-o", str(LIB), str(SRC / "engine.cu"),
+           str(SRC / "postproc.cu"), str(SRC / "plan_host.cpp")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     tmp = LIB.with_suffix(".so.tmp")

@@ -999,3 +999,26 @@ if __name__ == "__main__":
     if "--ms" in sys.argv:
         write_ms_file()
         print("wrote", MS_DATA_FILE)
+
+
+PHYSICS_FILE_MAGIC = b"GEGSPHY1"
+
+
+def write_physics_file(path, media, block):
+    """Write a physics block for C/C++ callers (read by gegs_plan_load,
+    include/gegs_plan.h): the magic "GEGSPHY1", the block size and the number
+    of media (uint32 each), each medium's name NUL-padded to 32 bytes, then the
+    block as it lies in memory. `media` names the block's media in index order."""
+    import struct
+    blk = np.ascontiguousarray(block)
+    nmed = int(np.asarray(blk["nmed"]).reshape(-1)[0])
+    if nmed != len(media):
+        raise ValueError(f"{len(media)} media names for a block of {nmed}")
+    with open(path, "wb") as f:
+        f.write(PHYSICS_FILE_MAGIC + struct.pack("<II", blk.dtype.itemsize, len(media)))
+        for m in media:
+            b = m.encode("ascii")
+            if len(b) >= 32:
+                raise ValueError(f"medium name {m!r} longer than 31 characters")
+            f.write(b + b"\0" * (32 - len(b)))
+        f.write(blk.tobytes())
