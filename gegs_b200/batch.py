@@ -49,11 +49,10 @@ def autotune(engine, job, sample=None, candidates=None, dimensions=None, rounds=
     With `candidates`, each is timed and the fastest kept. Otherwise a
     coordinate descent: starting from choose_options, each dimension of
     TUNE_DIMENSIONS (in-flight batch, grid blocks per SM, photon and electron
-    step budgets, refill threshold) tries its alternatives with the others
-    fixed and keeps any that is faster; `rounds` passes over the dimensions.
-    Dimensions: in-flight batch, grid blocks per SM, photon and electron step
-    budgets, refill threshold, and whether the photon tables are staged in
-    shared memory (GEGS_RUN_STAGE_TABLES).
+    step budgets, refill threshold, and whether the photon tables are staged
+    in shared memory, GEGS_RUN_STAGE_TABLES) tries its alternatives with the
+    others fixed and keeps any that is faster; `rounds` passes over the
+    dimensions.
     Every trial first runs a quarter sample untimed (graph build, queue
     sizing), then the timed sample; the tally is reset afterwards. `start`
     replaces choose_options' defaults (a batch within a memory share). Returns
