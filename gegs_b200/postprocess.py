@@ -10,6 +10,7 @@
 from __future__ import annotations
 
 import ctypes as C
+from fractions import Fraction
 from pathlib import Path
 
 import numpy as np
@@ -224,7 +225,8 @@ def relative_dose(dose, x_bounds, y_bounds, z_bounds, start, sizes, dims, measur
                 else:
                     pas = -1
         lines.append(f"{m:f}\t {calc[i]:f}\t {pas}")
-    pct = f"{count / total * 100:.0f}" if total else "nan"
+    # (float)count / total, times 100 in float, printed with %.0f
+    pct = f"{float(f(f(f(count) / f(total)) * f(100.0))):.0f}" if total else "nan"
     lines.append(f"Totally {total} points compared, {count} passed, percentage = {pct} %")
     return lines, total, count
 
@@ -237,14 +239,35 @@ def write_relative_dose(base, lines, dims):
     return name
 
 
+def strtof(tok):
+    """A decimal string rounded once, to the nearest float32 (ties to even),
+    as C's strtof and C++'s `stream >> float` round it. float() alone rounds
+    to double first, and the second rounding to float32 goes wrong where the
+    double lands exactly halfway between two float32 values."""
+    d = float(tok)
+    with np.errstate(over="ignore"):                # beyond the float range: infinity, as strtof gives
+        x = np.float32(d)
+        if not np.isfinite(x) or float(x) == d:
+            return x
+        lo, hi = (np.nextafter(x, np.float32(-np.inf)), x) if float(x) > d else (x, np.nextafter(x, np.float32(np.inf)))
+    mid = (float(lo) + float(hi)) / 2.0            # exact: two float32 values and a halving
+    if d != mid:
+        return x
+    exact, m = Fraction(tok.strip()), Fraction(mid)
+    if exact != m:
+        return hi if exact > m else lo
+    return lo if int(lo.view(np.uint32)) % 2 == 0 else hi
+
+
 def read_measured(path, n):
     """The measured data file: the first number of each of the first n lines
-    (the reference reads `infile >> v` then skips the rest of the line)."""
+    (the reference reads `infile >> v` into a float, output.c:641-676, then
+    skips the rest of the line)."""
     vals = []
     for line in Path(path).read_text().splitlines():
         tok = line.split()
         if tok:
-            vals.append(float(tok[0]))
+            vals.append(strtof(tok[0]))
         if len(vals) == n:
             break
     if len(vals) < n:
