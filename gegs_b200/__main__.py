@@ -85,7 +85,7 @@ def run_plan(ini, device=0, max_histories=None, out=sys.stdout, uncertainty_batc
             eng.run(int(f["hist_begin"]), int(f["hist_end"]))
             energy += eng.tally().astype(np.float64) * of
     wall = time.perf_counter() - t0
-    dose = energy * (2.0 ** -30) / job.voxel_mass() * plan.dose_unit
+    dose = F.dose_from_energy(energy * (2.0 ** -30), job.voxel_mass(), plan.dose_unit)
     Path(plan.output_dir).mkdir(parents=True, exist_ok=True)
     name = F.write_dose(plan.output_base, dose.astype(np.float32), plan.nx, plan.ny, plan.nz)
     st = eng.stats()

@@ -78,12 +78,14 @@ std::string read_text(const fs::path &p)
     return out;
 }
 
-double to_double(const std::string &t, const std::string &what)
+// A number as the reference reads it: into a float (`stream >> float`,
+// scanf's %f), rounded once from the decimal.
+float to_float(const std::string &t, const std::string &what)
 {
     const char *b = t.c_str();
     char *e = nullptr;
     errno = 0;
-    double v = std::strtod(b, &e);
+    float v = std::strtof(b, &e);
     if (e == b || *e != '\0') throw PlanError("could not parse " + what + " '" + t + "'");
     return v;
 }
@@ -135,15 +137,15 @@ struct Stream {
         i = m;
         return t;
     }
-    double num() { return to_double(token(), "number"); }
+    float num() { return to_float(token(), "number"); }
     long long num_int()
     {
         std::string t = token();
-        if (t.find_first_of(".eE") != std::string::npos) return (long long)to_double(t, "number");
+        if (t.find_first_of(".eE") != std::string::npos) return (long long)std::strtod(t.c_str(), nullptr);
         return std::stoll(t);
     }
     void chr() { skip_ws(); i++; }
-    double num_sep() { double v = num(); chr(); return v; }
+    float num_sep() { float v = num(); chr(); return v; }
     long long num_sep_int() { long long v = num_int(); chr(); return v; }
     bool find_line_starting(const std::string &title)
     {
@@ -211,7 +213,7 @@ bool ini_on(const Ini &ini, const std::string &sec, const std::string &key)
 std::vector<double> floats(const std::string &v, size_t n, const std::string &what)
 {
     std::vector<double> out;
-    for (const auto &t : split_ws(v)) out.push_back(to_double(t, what));
+    for (const auto &t : split_ws(v)) out.push_back(to_float(t, what));
     if (out.size() < n) throw PlanError(what + " needs " + std::to_string(n) + " numbers, got '" + v + "'");
     out.resize(n);
     return out;
@@ -288,7 +290,7 @@ Phantom read_egsphant(const fs::path &path)
     auto d = split_ws(r.s.substr(r.i));
     if (d.size() < nvox) throw PlanError(name + ": " + std::to_string(d.size()) + " densities for " + std::to_string(nvox) + " voxels");
     ph.density.resize(nvox);
-    for (size_t v = 0; v < nvox; v++) ph.density[v] = (float)to_double(d[v], "density");
+    for (size_t v = 0; v < nvox; v++) ph.density[v] = to_float(d[v], "density");
     return ph;
 }
 
@@ -335,20 +337,21 @@ void read_egsphsp1(const fs::path &path, std::vector<gegs_phsp_record> &out)
 }
 
 // ---- egsinp component modules (init.cu:345-689) -----------------------------
+// Every number is read into a float, as the reference reads it (`infile >> float`).
 struct Leaf {
-    double wl, wt, wg, wtip, wts, wbs, ztip, zl, zt, zg, zth, zbh, holepos, zts, zbs;
+    float wl, wt, wg, wtip, wts, wbs, ztip, zl, zt, zg, zth, zbh, holepos, zts, zbs;
 };
 
 struct DynVMLC {
-    double rmax, zmin, zthick, x_start, air_gap, rad_end;
+    float rmax, zmin, zthick, x_start, air_gap, rad_end;
     Leaf full, target, iso;
     long long n_full, n_half;
-    std::vector<std::tuple<double, double, long long>> open;
+    std::vector<std::tuple<float, float, long long>> open;
     std::string media;
 };
 
 struct SecJaws {
-    double rmax, zminy, zmaxy, zminx, zmaxx;
+    float rmax, zminy, zmaxy, zminx, zmaxx;
     std::string media;
 };
 
@@ -392,7 +395,7 @@ DynVMLC read_dynvmlc(const fs::path &path)
     r.ignore();
     long long total = 0;
     while (total < 60) {
-        double neg = r.num_sep(), pos = r.num_sep();
+        float neg = r.num_sep(), pos = r.num_sep();
         long long num = r.num_int();
         m.open.emplace_back(neg, pos, num);
         total += num;
@@ -421,128 +424,133 @@ SecJaws read_secjaws(const fs::path &path)
     return j;
 }
 
-// 14 (x, z) vertices of a leaf type (read_egsinp.h:40-88)
-void leaf_vertices(const Leaf &L, int kind, double zmin, double zthick, double v[14][2])
+// 14 (x, z) vertices of a leaf type, in float (read_egsinp.h:37-88)
+void leaf_vertices(const Leaf &L, int kind, float zmin, float zthick, float v[14][2])
 {
-    const double wl = L.wl, wt = L.wt, wg = L.wg, wtip = L.wtip, wts = L.wts, wbs = L.wbs, zmax = zmin + zthick;
+    const float wl = L.wl, wt = L.wt, wg = L.wg, wtip = L.wtip, wts = L.wts, wbs = L.wbs, zmax = zmin + zthick;
     if (kind == 0) {
-        const double t[14][2] = {{0, L.ztip}, {wtip, L.ztip}, {wtip, L.zl}, {wt + wl - wg, L.zl}, {wt + wl - wg, L.zg},
-                                 {wt + wl, L.zg}, {wt + wl, zmax}, {wt + wts - wbs, zmax}, {wt + wts - wbs, L.zbs},
-                                 {wt + wts, L.zbs}, {wt + wts, L.zts}, {wt, L.zts}, {wt, L.zt}, {0, L.zt}};
+        const float t[14][2] = {{0, L.ztip}, {wtip, L.ztip}, {wtip, L.zl}, {wt + wl - wg, L.zl}, {wt + wl - wg, L.zg},
+                                {wt + wl, L.zg}, {wt + wl, zmax}, {wt + wts - wbs, zmax}, {wt + wts - wbs, L.zbs},
+                                {wt + wts, L.zbs}, {wt + wts, L.zts}, {wt, L.zts}, {wt, L.zt}, {0, L.zt}};
         std::memcpy(v, t, sizeof t);
     } else if (kind == 1) {
-        const double t[14][2] = {{0, zmin}, {wt + wl - wbs + wts, zmin}, {wt + wl - wbs + wts, L.zts},
-                                 {wt + wl - wbs, L.zts}, {wt + wl - wbs, L.zbs}, {wt + wl, L.zbs}, {wt + wl, L.zg},
-                                 {wt + wl - wg, L.zg}, {wt + wl - wg, L.ztip}, {wt + wl - wg - wtip, L.ztip},
-                                 {wt + wl - wg - wtip, L.zl}, {wt, L.zl}, {wt, L.zt}, {0, L.zt}};
+        const float t[14][2] = {{0, zmin}, {wt + wl - wbs + wts, zmin}, {wt + wl - wbs + wts, L.zts},
+                                {wt + wl - wbs, L.zts}, {wt + wl - wbs, L.zbs}, {wt + wl, L.zbs}, {wt + wl, L.zg},
+                                {wt + wl - wg, L.zg}, {wt + wl - wg, L.ztip}, {wt + wl - wg - wtip, L.ztip},
+                                {wt + wl - wg - wtip, L.zl}, {wt, L.zl}, {wt, L.zt}, {0, L.zt}};
         std::memcpy(v, t, sizeof t);
     } else {
-        const double t[14][2] = {{0, L.zt}, {wt, L.zt}, {wt, L.ztip}, {wt + wtip, L.ztip}, {wt + wtip, L.zl},
-                                 {wt + wl - wg, L.zl}, {wt + wl - wg, L.zg}, {wt + wl, L.zg}, {wt + wl, zmax},
-                                 {wts - wbs, zmax}, {wts - wbs, L.zbs}, {wts, L.zbs}, {wts, L.zts}, {0, L.zts}};
+        const float t[14][2] = {{0, L.zt}, {wt, L.zt}, {wt, L.ztip}, {wt + wtip, L.ztip}, {wt + wtip, L.zl},
+                                {wt + wl - wg, L.zl}, {wt + wl - wg, L.zg}, {wt + wl, L.zg}, {wt + wl, zmax},
+                                {wts - wbs, zmax}, {wts - wbs, L.zbs}, {wts, L.zbs}, {wts, L.zts}, {0, L.zts}};
         std::memcpy(v, t, sizeof t);
     }
 }
 
-// crossXZ, boundaries and constants of the MLC (init.cu:345-611), leaf-end outline (init.cu:256-343)
+// The reference's leaf-end outline of bank A (leaf_end, init.cu:266-280),
+// bottom to top; the first and last depth are -/+ half the leaf thickness.
+const float kLeafEndX[15] = {-0.86708f, -0.64016f, -0.44640f, -0.28667f, -0.16167f, -0.07199f, -0.01802f, 0.0f,
+                             -0.01802f, -0.07199f, -0.16167f, -0.28667f, -0.44640f, -0.64016f, -0.86708f};
+const float kLeafEndY[15] = {0.0f, -2.92273f, -2.45316f, -1.97406f, -1.48729f, -0.99475f, -0.49834f, 0.0f,
+                             0.49834f, 0.99475f, 1.48729f, 1.97406f, 2.45316f, 2.92273f, 0.0f};
+
+// crossXZ, boundaries and constants of the MLC in float (read_egsinp,
+// init.cu:451-561), and the leaf-end outline (leaf_end, init.cu:256-343).
+// Entries the reference leaves unset (the 16th vertex of most leaves) are 0.
 void build_mlc(const DynVMLC &m, gegs_scene &S, float cross_yz[34][2])
 {
-    static double cross[960][2];
-    std::memset(cross, 0, sizeof cross);
-    const double zmin = m.zmin, zthick = m.zthick;
-    double vf[14][2], vt[14][2], vi[14][2];
+    std::memset(S.crossXZ, 0, sizeof S.crossXZ);
+    const float zmin = m.zmin, zthick = m.zthick, air_gap = m.air_gap;
+    float vf[14][2], vt[14][2], vi[14][2];
     leaf_vertices(m.full, 0, zmin, zthick, vf);
     leaf_vertices(m.target, 1, zmin, zthick, vt);
     leaf_vertices(m.iso, 2, zmin, zthick, vi);
-    double X = m.x_start;
+    float X = m.x_start;
     int i = 0;
-    auto put = [&](int i, double X, const double v[14][2]) {
+    auto put = [&](int i, float X, const float v[14][2]) {
         for (int k = 0; k < 14; k++) {
-            cross[i * 16 + k][0] = (X + v[k][0]) / zmin * v[k][1];
-            cross[i * 16 + k][1] = v[k][1];
+            S.crossXZ[i * 16 + k][0] = (X + v[k][0]) / zmin * v[k][1];
+            S.crossXZ[i * 16 + k][1] = v[k][1];
         }
     };
-    for (long long k = 0; k < m.n_full; k++) { put(i, X, vf); X += m.full.wl + m.air_gap; i++; }
-    const double x_mid_1 = X;
+    for (long long k = 0; k < m.n_full; k++) { put(i, X, vf); X = X + m.full.wl + air_gap; i++; }
+    const float x_mid_1 = X;
     for (long long k = 0; k < m.n_half / 2; k++) {
-        put(i, X, vt); X += m.target.wl + m.air_gap; i++;
-        put(i, X, vi); X += m.iso.wl + m.air_gap; i++;
+        put(i, X, vt); X = X + m.target.wl + air_gap; i++;
+        put(i, X, vi); X = X + m.iso.wl + air_gap; i++;
     }
-    const double x_mid_2 = X;
-    for (long long k = 0; k < m.n_full; k++) { put(i, X, vf); X += m.full.wl + m.air_gap; i++; }
-    const double x_end = X - m.air_gap + m.full.wg;
+    const float x_mid_2 = X;
+    for (long long k = 0; k < m.n_full; k++) { put(i, X, vf); X = X + m.full.wl + air_gap; i++; }
+    const float x_end = X - air_gap + m.full.wg;
     int kk = 0;
     for (const auto &row : m.open)
         for (long long q = 0; q < std::get<2>(row); q++, kk++)
-            if (kk < 60) { cross[14 + kk * 16][0] = std::get<0>(row); cross[14 + kk * 16][1] = std::get<1>(row); }
-    cross[15][0] = zmin; cross[15][1] = zthick;
-    cross[31][0] = m.x_start; cross[31][1] = x_end;
-    cross[47][0] = x_mid_1; cross[47][1] = x_mid_2;
-    cross[63][1] = m.air_gap;
-    cross[79][0] = m.full.wl; cross[79][1] = m.target.wl;
-    cross[95][0] = m.iso.wl; cross[95][1] = m.full.wt;
-    cross[111][0] = m.rmax;
-    for (int k = 0; k < 960; k++) { S.crossXZ[k][0] = (float)cross[k][0]; S.crossXZ[k][1] = (float)cross[k][1]; }
-    const double zmax = zmin + zthick;
-    const double bxz[4][2] = {{m.x_start / zmin * zmax, zmax}, {m.x_start, zmin}, {x_end, zmin}, {x_end / zmin * zmax, zmax}};
-    const double byz[4][2] = {{-m.rmax, zmax}, {-m.rmax, zmin}, {m.rmax, zmin}, {m.rmax, zmax}};
-    for (int k = 0; k < 4; k++)
-        for (int c = 0; c < 2; c++) { S.boundaryXZ[k][c] = (float)bxz[k][c]; S.boundaryYZ[k][c] = (float)byz[k][c]; }
-    S.mlc_rmax = (float)m.rmax; S.mlc_zmin = (float)zmin; S.mlc_zthick = (float)zthick;
-    S.mlc_x_start = (float)m.x_start; S.mlc_x_end = (float)x_end; S.mlc_x_mid_1 = (float)x_mid_1;
-    S.mlc_x_mid_2 = (float)x_mid_2; S.mlc_air_gap = (float)m.air_gap; S.mlc_wl_full = (float)m.full.wl;
-    S.mlc_wl_target = (float)m.target.wl; S.mlc_wl_isocenter = (float)m.iso.wl; S.mlc_wt = (float)m.full.wt;
-    // leaf-end outline: a circular end of radius rad_end sampled at 15 depths
-    const double zc = zthick / 2, R = m.rad_end;
-    double ys[15], xs[15], n[30][2], c[34][2];
-    const double step = (zc - (-zc)) / 14.0;
-    for (int k = 0; k < 15; k++) ys[k] = (double)k * step + (-zc);
-    ys[14] = zc;
-    for (int k = 0; k < 15; k++) xs[k] = -(R - std::sqrt(std::max(R * R - ys[k] * ys[k], 0.0)));
-    for (int k = 0; k < 15; k++) { n[k][0] = xs[k]; n[k][1] = ys[k]; n[29 - k][0] = -xs[k]; n[29 - k][1] = ys[k]; }
-    c[0][0] = -m.rmax; c[0][1] = zthick + zmin;
-    c[1][0] = -m.rmax; c[1][1] = zmin;
-    for (int k = 0; k < 15; k++) { c[2 + k][0] = n[k][0]; c[2 + k][1] = n[k][1] + zc + zmin; }
-    for (int k = 0; k < 15; k++) { c[17 + k][0] = n[15 + k][0]; c[17 + k][1] = n[15 + k][1] + zc + zmin; }
-    c[32][0] = m.rmax; c[32][1] = zmin;
-    c[33][0] = m.rmax; c[33][1] = zthick + zmin;
-    for (int k = 0; k < 34; k++) { cross_yz[k][0] = (float)c[k][0]; cross_yz[k][1] = (float)c[k][1]; }
+            if (kk < 60) { S.crossXZ[14 + kk * 16][0] = std::get<0>(row); S.crossXZ[14 + kk * 16][1] = std::get<1>(row); }
+    S.crossXZ[15][0] = zmin; S.crossXZ[15][1] = zthick;
+    S.crossXZ[31][0] = m.x_start; S.crossXZ[31][1] = x_end;
+    S.crossXZ[47][0] = x_mid_1; S.crossXZ[47][1] = x_mid_2;
+    S.crossXZ[63][1] = air_gap;
+    S.crossXZ[79][0] = m.full.wl; S.crossXZ[79][1] = m.target.wl;
+    S.crossXZ[95][0] = m.iso.wl; S.crossXZ[95][1] = m.full.wt;
+    S.crossXZ[111][0] = m.rmax;
+    const float ztop = zthick + zmin;
+    const float bxz[4][2] = {{m.x_start / zmin * (zmin + zthick), ztop}, {m.x_start, zmin}, {x_end, zmin},
+                             {x_end / zmin * (zmin + zthick), ztop}};
+    const float byz[4][2] = {{-m.rmax, ztop}, {-m.rmax, zmin}, {m.rmax, zmin}, {m.rmax, ztop}};
+    std::memcpy(S.boundaryXZ, bxz, sizeof bxz);
+    std::memcpy(S.boundaryYZ, byz, sizeof byz);
+    S.mlc_rmax = m.rmax; S.mlc_zmin = zmin; S.mlc_zthick = zthick;
+    S.mlc_x_start = m.x_start; S.mlc_x_end = x_end; S.mlc_x_mid_1 = x_mid_1;
+    S.mlc_x_mid_2 = x_mid_2; S.mlc_air_gap = air_gap; S.mlc_wl_full = m.full.wl;
+    S.mlc_wl_target = m.target.wl; S.mlc_wl_isocenter = m.iso.wl; S.mlc_wt = m.full.wt;
+    const float zc = zthick / 2;
+    float n[30][2];
+    for (int k = 0; k < 15; k++) {
+        const float y = k == 0 ? -zc : (k == 14 ? zc : kLeafEndY[k]);
+        n[k][0] = kLeafEndX[k]; n[k][1] = y;                       // bank A
+        n[29 - k][0] = std::fabs(kLeafEndX[k]); n[29 - k][1] = y;  // bank B, its mirror
+    }
+    cross_yz[0][0] = -m.rmax; cross_yz[0][1] = zthick + zmin;
+    cross_yz[1][0] = -m.rmax; cross_yz[1][1] = zmin;
+    for (int k = 0; k < 30; k++) { cross_yz[2 + k][0] = n[k][0]; cross_yz[2 + k][1] = n[k][1] + zc + zmin; }
+    cross_yz[32][0] = m.rmax; cross_yz[32][1] = zmin;
+    cross_yz[33][0] = m.rmax; cross_yz[33][1] = zthick + zmin;
 }
 
-// per-field jaw polygons (setup_secjaws, init.cu:1504-1592)
-void secjaws_polygons(const SecJaws &j, double x1, double x2, double y1, double y2, double sid, gegs_field &F)
+// per-field jaw polygons in float (setup_secjaws, init.cu:1504-1592)
+void secjaws_polygons(const SecJaws &j, float x1, float x2, float y1, float y2, float sid, gegs_field &F)
 {
-    const double bminy[4][2] = {{x1 * j.zminy / sid - 0.5, y1 * j.zminy / sid - 0.5}, {x2 * j.zminy / sid + 0.5, y1 * j.zminy / sid - 0.5},
-                                {x2 * j.zminy / sid + 0.5, y2 * j.zminy / sid + 0.5}, {x1 * j.zminy / sid - 0.5, y2 * j.zminy / sid + 0.5}};
-    const double bminx[4][2] = {{x1 * j.zminx / sid - 0.5, y1 * j.zminx / sid - 0.5}, {x2 * j.zminx / sid + 0.5, y1 * j.zminx / sid - 0.5},
-                                {x2 * j.zminx / sid + 0.5, y2 * j.zminx / sid + 0.5}, {x1 * j.zminx / sid - 0.5, y2 * j.zminx / sid + 0.5}};
-    const double bmaxy[4][2] = {{-j.rmax, j.zminy}, {j.rmax, j.zminy}, {j.rmax, j.zmaxy}, {-j.rmax, j.zmaxy}};
-    const double bmaxx[4][2] = {{-j.rmax, j.zminx}, {j.rmax, j.zminx}, {j.rmax, j.zmaxx}, {-j.rmax, j.zmaxx}};
-    const double gy[8][2] = {{-j.rmax, j.zmaxy}, {-j.rmax, j.zminy}, {y1 * j.zminy / sid, j.zminy}, {y1 * j.zmaxy / sid, j.zmaxy},
-                             {y2 * j.zmaxy / sid, j.zmaxy}, {y2 * j.zminy / sid, j.zminy}, {j.rmax, j.zminy}, {j.rmax, j.zmaxy}};
-    const double gx[8][2] = {{-j.rmax, j.zmaxx}, {-j.rmax, j.zminx}, {x1 * j.zminx / sid, j.zminx}, {x1 * j.zmaxx / sid, j.zmaxx},
-                             {x2 * j.zmaxx / sid, j.zmaxx}, {x2 * j.zminx / sid, j.zminx}, {j.rmax, j.zminx}, {j.rmax, j.zmaxx}};
-    for (int k = 0; k < 4; k++)
-        for (int c = 0; c < 2; c++) {
-            F.boundMinY[k][c] = (float)bminy[k][c]; F.boundMinX[k][c] = (float)bminx[k][c];
-            F.boundMaxY[k][c] = (float)bmaxy[k][c]; F.boundMaxX[k][c] = (float)bmaxx[k][c];
-        }
-    for (int k = 0; k < 8; k++)
-        for (int c = 0; c < 2; c++) { F.jawsGeomY[k][c] = (float)gy[k][c]; F.jawsGeomX[k][c] = (float)gx[k][c]; }
+    const float h = 0.5f;
+    const float bminy[4][2] = {{x1 * j.zminy / sid - h, y1 * j.zminy / sid - h}, {x2 * j.zminy / sid + h, y1 * j.zminy / sid - h},
+                               {x2 * j.zminy / sid + h, y2 * j.zminy / sid + h}, {x1 * j.zminy / sid - h, y2 * j.zminy / sid + h}};
+    const float bminx[4][2] = {{x1 * j.zminx / sid - h, y1 * j.zminx / sid - h}, {x2 * j.zminx / sid + h, y1 * j.zminx / sid - h},
+                               {x2 * j.zminx / sid + h, y2 * j.zminx / sid + h}, {x1 * j.zminx / sid - h, y2 * j.zminx / sid + h}};
+    const float bmaxy[4][2] = {{-j.rmax, j.zminy}, {j.rmax, j.zminy}, {j.rmax, j.zmaxy}, {-j.rmax, j.zmaxy}};
+    const float bmaxx[4][2] = {{-j.rmax, j.zminx}, {j.rmax, j.zminx}, {j.rmax, j.zmaxx}, {-j.rmax, j.zmaxx}};
+    const float gy[8][2] = {{-j.rmax, j.zmaxy}, {-j.rmax, j.zminy}, {y1 * j.zminy / sid, j.zminy}, {y1 * j.zmaxy / sid, j.zmaxy},
+                            {y2 * j.zmaxy / sid, j.zmaxy}, {y2 * j.zminy / sid, j.zminy}, {j.rmax, j.zminy}, {j.rmax, j.zmaxy}};
+    const float gx[8][2] = {{-j.rmax, j.zmaxx}, {-j.rmax, j.zminx}, {x1 * j.zminx / sid, j.zminx}, {x1 * j.zmaxx / sid, j.zmaxx},
+                            {x2 * j.zmaxx / sid, j.zmaxx}, {x2 * j.zminx / sid, j.zminx}, {j.rmax, j.zminx}, {j.rmax, j.zmaxx}};
+    std::memcpy(F.boundMinY, bminy, sizeof bminy);
+    std::memcpy(F.boundMinX, bminx, sizeof bminx);
+    std::memcpy(F.boundMaxY, bmaxy, sizeof bmaxy);
+    std::memcpy(F.boundMaxX, bmaxx, sizeof bmaxx);
+    std::memcpy(F.jawsGeomY, gy, sizeof gy);
+    std::memcpy(F.jawsGeomX, gx, sizeof gx);
 }
 
-// per-field leaf-end polygons (init_leaf_pos, init.cu:1594-1662): pair j is
-// moved by POS = pos[j] and NEG = -pos[j+60] (the reference's bank swap),
-// in float arithmetic
-void leaf_endnodes(const float cross_yz[34][2], const float pos[120], double zmin, double zthick, double sid, gegs_field &F)
+// per-field leaf-end polygons in float (init_leaf_pos, init.cu:1594-1662):
+// pair j is moved by POS = pos[j] and NEG = -pos[j+60] (the reference's bank
+// swap); a pair whose positions do not add up to more than 0 keeps the outline
+void leaf_endnodes(const float cross_yz[34][2], const float pos[120], float zmin, float zthick, float sid, gegs_field &F)
 {
-    const float zc = (float)(zmin + zthick / 2), fsid = (float)sid;
+    const float zc = zmin + zthick / 2;
     for (int j = 0; j < 60; j++) {
         for (int k = 0; k < 34; k++) { F.endnode[j][k][0] = cross_yz[k][0]; F.endnode[j][k][1] = cross_yz[k][1]; }
         if (pos[j] + pos[j + 60] > 0.0f) {
             const float POS = pos[j], NEG = -pos[j + 60];
-            for (int k = 2; k < 17; k++) F.endnode[j][k][0] = cross_yz[k][0] + NEG * zc / fsid;
-            for (int k = 17; k < 32; k++) F.endnode[j][k][0] = cross_yz[k][0] + POS * zc / fsid;
+            for (int k = 2; k < 17; k++) F.endnode[j][k][0] = cross_yz[k][0] + NEG * zc / sid;
+            for (int k = 17; k < 32; k++) F.endnode[j][k][0] = cross_yz[k][0] + POS * zc / sid;
         }
     }
 }
@@ -602,7 +610,7 @@ void load(gegs_plan &pl, const fs::path &ini_path_in, const fs::path &physics_pa
     const fs::path here = ini_path.parent_path();
     const std::string prefix = ini_req(ini, "General", "output prefix");
     const fs::path outdir = data_path(here, ini_req(ini, "General", "output directory"));
-    const double hpm = floats(ini_req(ini, "General", "histories"), 1, "histories")[0];
+    const float hpm = floats(ini_req(ini, "General", "histories"), 1, "histories")[0];
     const fs::path data_dir = data_path(here, ini_req(ini, "Data", "data directory"));
     auto data = [&](const std::string &n) { return data_path(data_dir, n); };
     const std::string default_medium = ini_opt(ini, "Data", "default medium", "AIR700ICRU");
@@ -616,7 +624,7 @@ void load(gegs_plan &pl, const fs::path &ini_path_in, const fs::path &physics_pa
     Phantom ph = read_egsphant(data(ini_req(ini, "Phantom", "egsphant file")));
     const bool change_xyz = lower(strip(ini_opt(ini, "Phantom", "change coordinate", "Yes"))) != "no";
     const auto iso = floats(ini_req(ini, "Phantom", "isocenter location"), 3, "isocenter location");
-    const double sid = floats(ini_req(ini, "Phantom", "source to isocenter"), 1, "source to isocenter")[0];
+    const float sid = floats(ini_req(ini, "Phantom", "source to isocenter"), 1, "source to isocenter")[0];
 
     SecJaws jaws{};
     DynVMLC mlc{};
@@ -648,7 +656,7 @@ void load(gegs_plan &pl, const fs::path &ini_path_in, const fs::path &physics_pa
     for (int k = 0; k < 5; k++) S.other_med[k] = (int32_t)(std::find(media.begin(), media.end(), other[k]) - media.begin());
     S.region_flags = GEGS_F_RAYLEIGH | GEGS_F_BOUND_COMPTON | GEGS_F_ATOMIC_RELAXATION | GEGS_F_PHOTO_ANGULAR;
     S.change_xyz = change_xyz ? 1 : 0;
-    S.source_to_isocenter = (float)sid;
+    S.source_to_isocenter = sid;
     for (int k = 0; k < 3; k++) S.iso[k] = (float)iso[k];
     // module order (CUDA_EGS.cu:1277-1305)
     int8_t order[8] = {0};
@@ -669,7 +677,7 @@ void load(gegs_plan &pl, const fs::path &ini_path_in, const fs::path &physics_pa
     if (pl.phsp.empty()) throw PlanError("the phase space holds no particles");
 
     // fields (read_mlcinfo / read_mlcinp, init.cu:1377-1500)
-    struct FieldInfo { double angle, x1, x2, y1, y2; long long mu; std::string mlcinp; };
+    struct FieldInfo { float angle, x1, x2, y1, y2; long long mu; std::string mlcinp; };
     std::vector<FieldInfo> finfo;
     const std::string *mlcinfo = ini_get(ini, "MLC", "mlcinfo file");
     if (mlc_on && !mlcinfo) throw PlanError("property \"mlcinfo file\" is not specified in the section \"MLC\"");
@@ -688,11 +696,13 @@ void load(gegs_plan &pl, const fs::path &ini_path_in, const fs::path &physics_pa
             finfo.push_back(f);
         }
     } else {
-        finfo.push_back(FieldInfo{0.0, -20.0, 20.0, -20.0, 20.0, 1, ""});
+        finfo.push_back(FieldInfo{0.0f, -20.0f, 20.0f, -20.0f, 20.0f, 1, ""});
     }
     if (finfo.empty()) throw PlanError("the mlcinfo file lists no fields");
     if ((int)finfo.size() > GEGS_MAX_FIELDS) throw PlanError("more fields than GEGS_MAX_FIELDS");
-    // output factors: interpolation in sqrt(field area), float32 as the package's reader (init.cu:1450-1466)
+    // output factors: interpolation in sqrt(field area), in float (read_mlcinp,
+    // init.cu:1449-1458); a field size outside the table leaves the reference's
+    // factor unset, 0 in its zero-initialised field array
     pl.output_factor.assign(finfo.size(), 1.0);
     if (ini_on(ini, "Output factor", "use output factor")) {
         Stream r(read_text(data(ini_req(ini, "Output factor", "output factor file"))));
@@ -700,10 +710,11 @@ void load(gegs_plan &pl, const fs::path &ini_path_in, const fs::path &physics_pa
         const long long n = r.num_int();
         r.ignore();
         std::vector<std::pair<float, float>> tab;
-        for (long long k = 0; k < n; k++) { float a = (float)r.num(), b = (float)r.num(); r.ignore(); tab.emplace_back(a, b); }
+        for (long long k = 0; k < n; k++) { float a = r.num(), b = r.num(); r.ignore(); tab.emplace_back(a, b); }
         for (size_t i = 0; i < finfo.size(); i++) {
             const FieldInfo &f = finfo[i];
-            const float size = (float)std::sqrt((f.x2 - f.x1) * (f.y2 - f.y1));
+            const float size = std::sqrt((f.x2 - f.x1) * (f.y2 - f.y1));
+            pl.output_factor[i] = 0.0;
             for (size_t j = 0; j + 1 < tab.size(); j++)
                 if (tab[j].first < size && size <= tab[j + 1].first) {
                     pl.output_factor[i] = (double)(tab[j].second + (size - tab[j].first) * (tab[j + 1].second - tab[j].second)
@@ -721,8 +732,10 @@ void load(gegs_plan &pl, const fs::path &ini_path_in, const fs::path &physics_pa
         if (max_hist > 0) n = std::min(n, max_hist);
         const uint64_t nrep = n > 0 ? (n - 1) / pl.phsp.size() : 0;
         if (nrep > 255) throw PlanError("more than 256 uses of each phase-space particle; add phase-space particles");
-        // gantry cos/sin as the reference uploads them (CUDA_EGS.cu:426-434)
-        const float a = (float)f.angle * (float)3.1415926 / 180.0f;
+        // gantry cos/sin as the reference uploads them (CUDA_EGS.cu:420-422): the
+        // angle times 3.1415926 / 180 in double, stored as a float; cos and sin
+        // of that float, correctly rounded
+        const float a = (float)((double)f.angle * 3.1415926 / 180);
         F.cos_angle = (float)std::cos((double)a);
         F.sin_angle = (float)std::sin((double)a);
         F.hist_begin = h; F.hist_end = h + n;
@@ -744,10 +757,10 @@ void load(gegs_plan &pl, const fs::path &ini_path_in, const fs::path &physics_pa
     S.nphsp = pl.phsp.size();
     S.hownear_region_offset = 5;
     S.seed = 0x6E65;
-    pl.dose_unit = 1.6e-8;
+    pl.dose_unit = 1.6e-8f;                              // a float (CUDA_EGS.h:536)
     if (ini_on(ini, "Calibration", "dose calibration")) {
-        const double hpc = floats(ini_req(ini, "Calibration", "histories per cGy"), 1, "histories per cGy")[0];
-        pl.dose_unit = 1.6e-8 * hpc / hpm;
+        const float hpc = floats(ini_req(ini, "Calibration", "histories per cGy"), 1, "histories per cGy")[0];
+        pl.dose_unit = 1.6e-8f * hpc / hpm;              // in float (CUDA_EGS.cu:1478)
     }
     pl.output_base = (outdir / prefix).string();
 }
@@ -794,31 +807,31 @@ double gegs_plan_output_factor(const gegs_plan *p, int32_t field)
     return p->output_factor[(size_t)field];
 }
 
-gegs_status gegs_plan_voxel_mass(const gegs_plan *p, double *mass, uint64_t nvox)
+gegs_status gegs_plan_voxel_mass(const gegs_plan *p, float *mass, uint64_t nvox)
 {
     if (!p || !mass || nvox != p->med.size()) return GEGS_ERR_ARG;
     const int nx = p->scene.nx, ny = p->scene.ny, nz = p->scene.nz;
-    for (int z = 0; z < nz; z++) {
-        const double dz = std::fabs((double)p->zb[z + 1] - (double)p->zb[z]);
-        for (int y = 0; y < ny; y++) {
-            const double dy = std::fabs((double)p->yb[y + 1] - (double)p->yb[y]);
+    for (int z = 0; z < nz; z++)
+        for (int y = 0; y < ny; y++)
             for (int x = 0; x < nx; x++) {
-                const double dx = std::fabs((double)p->xb[x + 1] - (double)p->xb[x]);
+                // (dx * dy) * dz in float, made positive, times the density (init.cu:1256-1271)
+                float vol = (p->xb[x + 1] - p->xb[x]) * (p->yb[y + 1] - p->yb[y]) * (p->zb[z + 1] - p->zb[z]);
+                if (vol < 0) vol = -vol;
                 const size_t v = ((size_t)z * ny + y) * nx + x;
-                double m = dz * dy * dx * (double)p->density[v];
-                mass[v] = m == 0.0 ? 1.0 : m;
+                const float m = vol * p->density[v];
+                mass[v] = m == 0.0f ? 1.0f : m;
             }
-        }
-    }
     return GEGS_OK;
 }
 
 gegs_status gegs_plan_dose(const gegs_plan *p, const int64_t *tally, float *dose, uint64_t nvox)
 {
     if (!p || !tally || !dose || nvox != p->med.size()) return GEGS_ERR_ARG;
-    std::vector<double> mass(nvox);
+    std::vector<float> mass(nvox);
     gegs_plan_voxel_mass(p, mass.data(), nvox);
-    for (uint64_t v = 0; v < nvox; v++) dose[v] = (float)((double)tally[v] * 9.313225746154785e-10 / mass[v] * p->dose_unit);
+    const float unit = (float)p->dose_unit;
+    // (float)E / mass * dose_unit in float, E the energy in MeV (write_dose, output.c:887-891)
+    for (uint64_t v = 0; v < nvox; v++) dose[v] = (float)((double)tally[v] * 9.313225746154785e-10) / mass[v] * unit;
     return GEGS_OK;
 }
 

@@ -23,6 +23,7 @@ from __future__ import annotations
 import os
 import re
 import struct
+from fractions import Fraction
 from pathlib import Path
 
 import numpy as np
@@ -34,6 +35,40 @@ from .scene import PHSP_DTYPE
 # a C++-istream-like reader
 # ---------------------------------------------------------------------------
 _NUM = re.compile(r"[+-]?(\d+\.?\d*|\.\d+)([eE][+-]?\d+)?")
+
+
+def strtof(tok):
+    """A decimal string rounded once, to the nearest float32 (ties to even),
+    as the reference's readers round it (`stream >> float`, `%f` in scanf).
+    float() alone rounds to double first, and rounding that double to float32
+    goes wrong where it lands exactly halfway between two float32 values."""
+    d = float(tok)
+    with np.errstate(over="ignore"):                # beyond the float range: infinity, as strtof gives
+        x = np.float32(d)
+        if not np.isfinite(x) or float(x) == d:
+            return x
+        lo, hi = (np.nextafter(x, np.float32(-np.inf)), x) if float(x) > d else (x, np.nextafter(x, np.float32(np.inf)))
+    mid = (float(lo) + float(hi)) / 2.0            # exact: two float32 values and a halving
+    if d != mid:
+        return x
+    exact, m = Fraction(tok.strip()), Fraction(mid)
+    if exact != m:
+        return hi if exact > m else lo
+    return lo if int(lo.view(np.uint32)) % 2 == 0 else hi
+
+
+def strtof_array(tokens):
+    """strtof over a list of decimal strings, vectorised: parsed as doubles,
+    rounded to float32, and only the values that landed on a float32 midpoint
+    (a double-rounding case) parsed again exactly."""
+    d = np.array(tokens, np.float64)
+    with np.errstate(over="ignore"):
+        x = d.astype(np.float32)
+        up = np.nextafter(x, np.where(x.astype(np.float64) < d, np.float32(np.inf), np.float32(-np.inf)))
+    tie = np.isfinite(x) & (x.astype(np.float64) != d) & ((x.astype(np.float64) + up.astype(np.float64)) / 2.0 == d)
+    for i in np.flatnonzero(tie):
+        x[i] = strtof(tokens[i])
+    return x
 
 
 class StreamReader:
@@ -71,7 +106,9 @@ class StreamReader:
             raise ValueError(f"expected a number at offset {self.i}: {self.s[self.i:self.i + 30]!r}")
         self.i = m.end()
         txt = m.group(0)
-        return int(float(txt)) if kind is int and any(c in txt for c in ".eE") else kind(txt)
+        if kind is int:
+            return int(float(txt)) if any(c in txt for c in ".eE") else int(txt)
+        return float(strtof(txt)) if kind is float else kind(txt)
 
     def char(self):
         self._skip_ws()
@@ -146,11 +183,11 @@ def read_egsphant(path):
                 raise ValueError(f"{path}: medium number outside 1..{nmed} (y={y}, z={z})")
             base = z * nx * ny + y * nx
             med[base:base + nx] = vals - 1
-    dens = np.array(rest.s[rest.i:].split(), np.float64)
-    if dens.size < nx * ny * nz:
-        raise ValueError(f"{path}: {dens.size} densities for {nx * ny * nz} voxels")
+    toks = rest.s[rest.i:].split()
+    if len(toks) < nx * ny * nz:
+        raise ValueError(f"{path}: {len(toks)} densities for {nx * ny * nz} voxels")
     return dict(media=media, nx=nx, ny=ny, nz=nz, x_bounds=xb, y_bounds=yb, z_bounds=zb,
-                voxel_med=med, density=dens[:nx * ny * nz].astype(np.float32))
+                voxel_med=med, density=strtof_array(toks[:nx * ny * nz]))
 
 
 def write_egsphant(path, media, x_bounds, y_bounds, z_bounds, voxel_med, density, estepe=1.0):
@@ -424,18 +461,29 @@ def read_output_factors(path):
 
 
 def output_factor(table, x1, x2, y1, y2):
-    """Linear interpolation in sqrt(field area); 1 when outside the table (init.cu:1450-1466)."""
-    size = float(np.sqrt((x2 - x1) * (y2 - y1)))
-    for j in range(len(table) - 1):
-        if table[j, 0] < size <= table[j + 1, 0]:
-            return float(table[j, 1] + (size - table[j, 0]) * (table[j + 1, 1] - table[j, 1])
-                         / (table[j + 1, 0] - table[j, 0]))
-    return 1.0
+    """Linear interpolation in sqrt(field area), in float (read_mlcinp,
+    init.cu:1449-1458). A field size outside the table leaves the reference's
+    factor unset, which is 0 in its zero-initialised field array; None here,
+    for the caller to report and apply as 0."""
+    f = np.float32
+    tab = np.asarray(table, np.float32)
+    size = np.sqrt((f(x2) - f(x1)) * (f(y2) - f(y1)))
+    for j in range(len(tab) - 1):
+        if tab[j, 0] < size <= tab[j + 1, 0]:
+            return float(tab[j, 1] + (size - tab[j, 0]) * (tab[j + 1, 1] - tab[j, 1]) / (tab[j + 1, 0] - tab[j, 0]))
+    return None
 
 
 # ---------------------------------------------------------------------------
 # dose output
 # ---------------------------------------------------------------------------
+def dose_from_energy(energy, voxel_mass, dose_unit):
+    """Dose per voxel in float32 from the energy in MeV (double), as write_dose
+    computes it (output.c:887-891): (float)E / mass * dose_unit, in float."""
+    e = np.asarray(energy, np.float64).astype(np.float32)
+    return (e / np.asarray(voxel_mass, np.float32)) * np.float32(dose_unit)
+
+
 def dose_file_name(base, nx, ny, nz):
     return f"{base}_DoseResults_{nx:03d}x{ny:03d}x{nz:03d}.bin"
 

@@ -77,8 +77,10 @@ def _on(v, default=False):
 
 
 def _floats(v, n, what):
+    """The first n numbers of an INI value, each rounded once to float, as the
+    reference's sscanf("%f") reads them (CUDA_EGS.cu:1076-1680)."""
     try:
-        vals = [float(t) for t in v.split()]
+        vals = [float(F.strtof(t)) for t in v.split()]
     except (AttributeError, ValueError):
         raise PlanError(f"could not parse {what} {v!r}")
     if len(vals) < n:
@@ -184,6 +186,11 @@ def load_plan(ini_path, seed=SEED_BASE, max_histories=None) -> Plan:
     if _on(_get(ini, "Output factor", "use output factor")):
         tab = F.read_output_factors(data(_get(ini, "Output factor", "output factor file", required=True)))
         ofac = [F.output_factor(tab, f["x1"], f["x2"], f["y1"], f["y2"]) for f in finfo]
+        for k, of in enumerate(ofac):
+            if of is None:
+                log.append(f"field {k + 1}: field size outside the output-factor table; its output factor is 0, "
+                           "as the reference leaves it")
+        ofac = [0.0 if of is None else of for of in ofac]
     mg = mlc.build() if mlc else None
     fields, h = [], 0
     for f in finfo:
@@ -205,10 +212,12 @@ def load_plan(ini_path, seed=SEED_BASE, max_histories=None) -> Plan:
         h += n
     beam = dict(change_xyz=change_xyz, source_to_isocenter=sid, iso=tuple(iso), z_phsp=z_phsp,
                 module_order=G.module_order(secjaws_on, mlc_on), mlc=mg)
-    dose_unit = DOSE_UNIT
+    # dose_unit is a float in the reference (CUDA_EGS.h:536), scaled in float (CUDA_EGS.cu:1478)
+    f32 = np.float32
+    dose_unit = float(f32(DOSE_UNIT))
     if _on(_get(ini, "Calibration", "dose calibration")):
         hpc = _floats(_get(ini, "Calibration", "histories per cGy", required=True), 1, "histories per cGy")[0]
-        dose_unit = DOSE_UNIT * hpc / hpm
+        dose_unit = float(f32(DOSE_UNIT) * f32(hpc) / f32(hpm))
     post = {}
     if _on(_get(ini, "Interpolation", "do interpolate")):
         post["interp"] = dict(
@@ -227,7 +236,7 @@ def load_plan(ini_path, seed=SEED_BASE, max_histories=None) -> Plan:
         gl, gd = _floats(_get(ini, "Dose output", "gamma index (mm,%)", required=True), 2, "gamma index (mm,%)")
         meas = _get(ini, "Dose output", "measured data", required=True)
         post["relative"] = dict(
-            start=[start[k] + iso[k] for k in range(3)],
+            start=[float(np.float32(start[k]) + np.float32(iso[k])) for k in range(3)],    # float sum (CUDA_EGS.cu:1617-1619)
             dims=[int(v) for v in _floats(_get(ini, "Dose output", "xyz dimensions", required=True), 3,
                                           "xyz dimensions")],
             sizes=_floats(_get(ini, "Dose output", "3d voxel sizes", required=True), 3, "3d voxel sizes"),

@@ -10,12 +10,12 @@
 from __future__ import annotations
 
 import ctypes as C
-from fractions import Fraction
 from pathlib import Path
 
 import numpy as np
 
 from .engine import load_library
+from .io_formats import strtof
 
 _ready = False
 
@@ -237,26 +237,6 @@ def write_relative_dose(base, lines, dims):
     with open(name, "w") as fh:
         fh.write("\n".join(lines) + "\n")
     return name
-
-
-def strtof(tok):
-    """A decimal string rounded once, to the nearest float32 (ties to even),
-    as C's strtof and C++'s `stream >> float` round it. float() alone rounds
-    to double first, and the second rounding to float32 goes wrong where the
-    double lands exactly halfway between two float32 values."""
-    d = float(tok)
-    with np.errstate(over="ignore"):                # beyond the float range: infinity, as strtof gives
-        x = np.float32(d)
-        if not np.isfinite(x) or float(x) == d:
-            return x
-        lo, hi = (np.nextafter(x, np.float32(-np.inf)), x) if float(x) > d else (x, np.nextafter(x, np.float32(np.inf)))
-    mid = (float(lo) + float(hi)) / 2.0            # exact: two float32 values and a halving
-    if d != mid:
-        return x
-    exact, m = Fraction(tok.strip()), Fraction(mid)
-    if exact != m:
-        return hi if exact > m else lo
-    return lo if int(lo.view(np.uint32)) % 2 == 0 else hi
 
 
 def read_measured(path, n):

@@ -46,10 +46,13 @@ class Job:
                            hownear_region_offset=hownear_region_offset)
 
     def voxel_mass(self):
+        """Voxel masses in g, float32, as the reference computes them from the
+        egsphant (init.cu:1256-1271): (dx * dy) * dz in float, made positive,
+        times the density; 0 becomes 1."""
         p = self.phantom
-        dx, dy, dz = (np.abs(np.diff(np.asarray(p[k], np.float64))) for k in ("x_bounds", "y_bounds", "z_bounds"))
-        vol = dz[:, None, None] * dy[None, :, None] * dx[None, None, :]
-        m = vol.reshape(-1) * p["density"].reshape(-1).astype(np.float64)
+        dx, dy, dz = (np.diff(np.asarray(p[k], np.float32)) for k in ("x_bounds", "y_bounds", "z_bounds"))
+        vol = np.abs((dx[None, None, :] * dy[None, :, None]) * dz[:, None, None])
+        m = (vol.reshape(-1) * np.asarray(p["density"], np.float32).reshape(-1)).astype(np.float32)
         m[m == 0] = 1.0
         return m
 

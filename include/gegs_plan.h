@@ -62,15 +62,17 @@ const gegs_physics *gegs_plan_physics(const gegs_plan *p);
 const gegs_scene *gegs_plan_scene(const gegs_plan *p);
 uint64_t gegs_plan_histories(const gegs_plan *p);     /* all fields: run [0, histories) */
 uint64_t gegs_plan_nvox(const gegs_plan *p);
-double gegs_plan_dose_unit(const gegs_plan *p);       /* cGy per MeV/g, calibration included */
+double gegs_plan_dose_unit(const gegs_plan *p);       /* cGy per MeV/g, calibration included (a float value) */
 int32_t gegs_plan_nfields(const gegs_plan *p);
-double gegs_plan_output_factor(const gegs_plan *p, int32_t field);   /* 1 unless [Output factor] is on */
+double gegs_plan_output_factor(const gegs_plan *p, int32_t field);   /* 1 unless [Output factor] is on;
+                                                                        0 for a field size outside its table */
 
-/* The voxel masses in g (|dx dy dz| * density, 0 taken as 1; init.cu:1256-1271), nvox doubles. */
-gegs_status gegs_plan_voxel_mass(const gegs_plan *p, double *mass, uint64_t nvox);
+/* The voxel masses in g, in float as the reference computes them: |(dx dy) dz| * density, 0 taken
+ * as 1 (init.cu:1256-1271); nvox floats. */
+gegs_status gegs_plan_voxel_mass(const gegs_plan *p, float *mass, uint64_t nvox);
 
-/* Dose per voxel from the int64 tally (MeV * 2^30), as the CLI computes it:
- * float(tally * 2^-30 / mass * dose_unit), the arithmetic in double. */
+/* Dose per voxel from the int64 tally (MeV * 2^30), as the reference's write_dose computes it
+ * from the energy E (output.c:887-891): (float)E / mass * dose_unit, in float. */
 gegs_status gegs_plan_dose(const gegs_plan *p, const int64_t *tally, float *dose, uint64_t nvox);
 
 /* Write <output directory>/<output prefix>_DoseResults_NNNxNNNxNNN.bin (raw

@@ -17,6 +17,11 @@ int ref_probe_uphi(int which, float a, float b, gegs_probe_particle *p, float *c
 int ref_probe_stage(int stage, uint32_t n, const gegs_probe_particle *in, const float *u, const uint32_t *un,
                     uint32_t ucap, gegs_probe_particle *out, uint32_t ocap, uint32_t *on, uint32_t *dreg, float *de,
                     uint32_t dcap, uint32_t *dn, uint32_t *used);
+/* host set-up: the reference's readers on plan files (init.cu); outfac_file NULL = off */
+int ref_setup_run(const char *egsphant, const char *mlc_egsinp, const char *jaws_egsinp, const char *mlcinfo,
+                  const char *data_directory, const char *outfac_file, float sid, const char *default_medium,
+                  char *msg, size_t msg_len);
+long ref_setup_get(const char *name, int field, void *dst, size_t bytes);
 #ifdef __cplusplus
 }
 #endif

@@ -416,3 +416,174 @@ extern "C" int ref_probe_stage(int stage, uint32_t n, const gegs_probe_particle 
     }
     return overruns;
 }
+
+// ---------------------------------------------------------------------------
+// Host set-up: the reference's own readers and geometry set-up (init.cu),
+// run on plan files, so tests can compare the scene this package builds from
+// the same files. The media tables and the region set-up are not needed for
+// that: init_media and init_regions stand in for media.cu:1294 and
+// init.cu:909 and keep what init_phantom_and_MLC hands them.
+// ---------------------------------------------------------------------------
+struct medium_t;
+
+static std::vector<std::string> g_setup_media;
+static std::vector<int> g_setup_media_idx;
+static std::vector<float> g_setup_density;
+static int g_setup_other[max_oth_med];
+static std::string g_setup_error;
+
+struct ref_setup_failure {};
+
+medium_t **init_media(uint nmed, string *media_names)
+{
+    g_setup_media.assign(media_names, media_names + nmed);
+    return (medium_t **)calloc(1, sizeof(medium_t *));
+}
+
+void init_regions(uint nreg, medium_t **, int *media_indices, float *densities, int *other_med_IDs)
+{
+    g_setup_media_idx.assign(media_indices, media_indices + nreg);
+    g_setup_density.assign(densities, densities + nreg);
+    std::memcpy(g_setup_other, other_med_IDs, sizeof g_setup_other);
+}
+
+void logstr(const char *, ...) {}
+
+void error(int ret, const char *format, ...)
+{
+    char buf[512];
+    va_list a;
+    va_start(a, format);
+    std::vsnprintf(buf, sizeof buf, format, a);
+    va_end(a);
+    g_setup_error = "error " + std::to_string(ret) + ": " + buf;
+    throw ref_setup_failure{};
+}
+
+void ce(int) {}
+void ce(int, const char *, ...) {}
+
+#include "commonBlocks host.h"   // h_nmed and the range-rejection arrays that init_phantom_and_MLC sets
+#include "ref_setup.inc"
+
+static void ref_gantry_one(uint iField, float *c, float *s)
+{
+#include "ref_gantry.inc"
+    *c = h_cosAngle;
+    *s = h_sinAngle;
+}
+
+struct ref_setup_field {
+    float angle, x1, x2, y1, y2, mu, output_factor, cos_angle, sin_angle, angle_rad;
+    float pos[TOTAL_MLC_LEAF];
+    point2D jaws[32];            // boundMinY, boundMinX, boundMaxY, boundMaxX (4 each), jawsGeomY, jawsGeomX (8 each)
+    point2D endnode[TOTAL_MLC_LEAF / 2][34];
+};
+static std::vector<ref_setup_field> g_setup_fields;
+static std::vector<float> g_setup_bounds[3];
+static std::vector<float> g_setup_mass;
+
+extern "C" int ref_setup_run(const char *egsphant, const char *mlc_egsinp, const char *jaws_egsinp,
+                             const char *mlcinfo, const char *data_directory, const char *outfac_file, float sid,
+                             const char *default_medium, char *msg, size_t msg_len)
+{
+    static std::string s_phant, s_mlc, s_jaws, s_info, s_dir, s_of;
+    s_phant = egsphant; s_mlc = mlc_egsinp; s_jaws = jaws_egsinp; s_info = mlcinfo; s_dir = data_directory;
+    s_of = outfac_file ? outfac_file : "";
+    egsphant_file = s_phant.c_str();
+    egsinp_file = s_mlc.c_str();
+    secjaws_file = s_jaws.c_str();
+    mlcinfo_file = s_info.c_str();
+    data_dir = s_dir.c_str();
+    output_factor_file = s_of.c_str();
+    outfac_on = outfac_file != nullptr;
+    h_SourceToIsocenter = sid;
+    Block_on = false;
+    Wedge_on = false;
+    GPUNo = 1;
+    g_setup_error.clear();
+    g_setup_fields.clear();
+    try {
+        init_phantom_and_MLC(string(default_medium));
+        for (int k = 0; k < 3; k++) {
+            const float *b = k == 0 ? d_phantom_x_bounds[0] : k == 1 ? d_phantom_y_bounds[0] : d_phantom_z_bounds[0];
+            const uint n = (k == 0 ? h_phantom_N.x : k == 1 ? h_phantom_N.y : h_phantom_N.z) + 1;
+            g_setup_bounds[k].assign(b, b + n);
+        }
+        g_setup_mass.assign(voxel_mass, voxel_mass + h_size_phantom);
+        read_mlcinp();
+        for (int i = 0; i < N_Field; i++) {
+            ref_setup_field F;
+            F.angle = field[i].angle; F.x1 = field[i].x1; F.x2 = field[i].x2; F.y1 = field[i].y1;
+            F.y2 = field[i].y2; F.mu = (float)field[i].MU; F.output_factor = field[i].output_factor;
+            std::memcpy(F.pos, field[i].pos, sizeof F.pos);
+            setup_secjaws(i);
+            std::memcpy(F.jaws + 0, boundMinY, sizeof boundMinY);
+            std::memcpy(F.jaws + 4, boundMinX, sizeof boundMinX);
+            std::memcpy(F.jaws + 8, boundMaxY, sizeof boundMaxY);
+            std::memcpy(F.jaws + 12, boundMaxX, sizeof boundMaxX);
+            std::memcpy(F.jaws + 16, jawsGeomY, sizeof jawsGeomY);
+            std::memcpy(F.jaws + 24, jawsGeomX, sizeof jawsGeomX);
+            init_leaf_pos(i);
+            for (int j = 0; j < TOTAL_MLC_LEAF / 2; j++) std::memcpy(F.endnode[j], endnode[j], 34 * sizeof(point2D));
+            ref_gantry_one(i, &F.cos_angle, &F.sin_angle);     // turns field[i].angle into radians, as the reference does
+            F.angle_rad = field[i].angle;
+            g_setup_fields.push_back(F);
+        }
+    } catch (const ref_setup_failure &) {
+        if (msg && msg_len) std::snprintf(msg, msg_len, "%s", g_setup_error.c_str());
+        return 1;
+    }
+    return 0;
+}
+
+// Copy one named result of ref_setup_run into dst (at most `bytes`); returns
+// the size of the result in bytes, or -1 for an unknown name or field.
+extern "C" long ref_setup_get(const char *name, int f, void *dst, size_t bytes)
+{
+    std::string n(name);
+    const void *src = nullptr;
+    size_t size = 0;
+    std::string names;
+    float mlc[12];
+    int dims[3];
+    float jaws[5];
+    if (n == "dims") { dims[0] = h_phantom_N.x; dims[1] = h_phantom_N.y; dims[2] = h_phantom_N.z; src = dims; size = sizeof dims; }
+    else if (n == "x_bounds" || n == "y_bounds" || n == "z_bounds") {
+        const auto &v = g_setup_bounds[n[0] - 'x'];
+        src = v.data(); size = v.size() * sizeof(float);
+    }
+    else if (n == "voxel_mass") { src = g_setup_mass.data(); size = g_setup_mass.size() * sizeof(float); }
+    else if (n == "media_index") { src = g_setup_media_idx.data(); size = g_setup_media_idx.size() * sizeof(int); }
+    else if (n == "density") { src = g_setup_density.data(); size = g_setup_density.size() * sizeof(float); }
+    else if (n == "other_med") { src = g_setup_other; size = sizeof g_setup_other; }
+    else if (n == "media") {
+        for (auto &m : g_setup_media) names += m + "\n";
+        src = names.data(); size = names.size();
+    }
+    else if (n == "mlc") {
+        const float v[12] = {MLC_rmax, MLC_zmin, MLC_zthick, MLC_x_start, MLC_x_end, MLC_x_mid_1, MLC_x_mid_2,
+                             MLC_air_gap, MLC_wl_full, MLC_wl_target, MLC_wl_isocenter, MLC_wt};
+        std::memcpy(mlc, v, sizeof mlc); src = mlc; size = sizeof mlc;
+    }
+    else if (n == "crossXZ") { src = crossXZ; size = sizeof crossXZ; }
+    else if (n == "boundaryXZ") { src = boundaryXZ; size = sizeof boundaryXZ; }
+    else if (n == "boundaryYZ") { src = boundaryYZ; size = sizeof boundaryYZ; }
+    else if (n == "crossYZ") { src = h_crossYZ; size = sizeof h_crossYZ; }
+    else if (n == "secjaws") {
+        jaws[0] = SecJaws.rmax; jaws[1] = SecJaws.zminy; jaws[2] = SecJaws.zmaxy; jaws[3] = SecJaws.zminx;
+        jaws[4] = SecJaws.zmaxx; src = jaws; size = sizeof jaws;
+    }
+    else if (n == "nfields") { dims[0] = (int)g_setup_fields.size(); src = dims; size = sizeof(int); }
+    else if (n == "field" || n == "pos" || n == "jaws" || n == "endnode") {
+        if (f < 0 || f >= (int)g_setup_fields.size()) return -1;
+        const ref_setup_field &F = g_setup_fields[f];
+        if (n == "field") { src = &F.angle; size = 10 * sizeof(float); }
+        else if (n == "pos") { src = F.pos; size = sizeof F.pos; }
+        else if (n == "jaws") { src = F.jaws; size = sizeof F.jaws; }
+        else { src = F.endnode; size = sizeof F.endnode; }
+    }
+    else return -1;
+    if (dst) std::memcpy(dst, src, size < bytes ? size : bytes);
+    return (long)size;
+}

@@ -80,4 +80,16 @@ typedef int cudaError_t;
 typedef void *cudaStream_t;
 typedef void *cudaEvent_t;
 
+/* The host set-up routines (init.cu) move their results with these. Device
+ * memory is host memory here, and a __constant__ symbol a plain global. */
+enum cudaMemcpyKind { cudaMemcpyHostToHost, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, cudaMemcpyDeviceToDevice };
+template <class T> static inline cudaError_t cudaMalloc(T **p, size_t n) { *p = (T *)std::malloc(n); return 0; }
+static inline cudaError_t cudaMemcpy(void *d, const void *s, size_t n, cudaMemcpyKind) { std::memcpy(d, s, n); return 0; }
+template <class T> static inline cudaError_t cudaMemcpyToSymbol(T &sym, const void *s, size_t n)
+{
+    std::memcpy((void *)&sym, s, n);
+    return 0;
+}
+static inline cudaError_t cudaSetDevice(int) { return 0; }
+
 #endif

@@ -70,6 +70,9 @@ def lib():
         L.ref_probe_uphi.argtypes = [C.c_int, C.c_float, C.c_float, vp, vp, C.c_float]
         L.ref_probe_stage.argtypes = [C.c_int, C.c_uint32, vp, vp, vp, C.c_uint32, vp, C.c_uint32, vp, vp, vp,
                                       C.c_uint32, vp, vp]
+        L.ref_setup_run.argtypes = [C.c_char_p] * 6 + [C.c_float, C.c_char_p, C.c_char_p, C.c_size_t]
+        L.ref_setup_get.argtypes = [C.c_char_p, C.c_int, vp, C.c_size_t]
+        L.ref_setup_get.restype = C.c_long
         _lib = L
     return _lib
 
@@ -189,3 +192,39 @@ def sort_by_stack(out, on):
     """Pushed particles of one probe as a list sorted by stack, push order kept."""
     rows = out[:int(on)]
     return rows[np.argsort(rows["status"], kind="stable")]
+
+
+class Setup:
+    """The reference's host set-up run on plan files: init_phantom_and_MLC
+    (the egsphant, the SECJAWS and DYNVMLC blocks of the egsinp files),
+    read_mlcinp (the mlcinfo field list and the mlcinp leaf positions) and,
+    per field, setup_secjaws, init_leaf_pos and the gantry cosine and sine
+    (init.cu:256-906, 1164-1662; CUDA_EGS.cu:420-422)."""
+
+    FIELD = ("angle", "x1", "x2", "y1", "y2", "mu", "output_factor", "cos_angle", "sin_angle", "angle_rad")
+
+    def __init__(self, egsphant, mlc_egsinp, jaws_egsinp, mlcinfo, data_dir, sid, default_medium,
+                 output_factor_file=None):
+        L = lib()
+        msg = C.create_string_buffer(512)
+        d = str(data_dir).rstrip("/") + "/"          # the reference prepends it to each mlcinp name
+        st = L.ref_setup_run(str(egsphant).encode(), str(mlc_egsinp).encode(), str(jaws_egsinp).encode(),
+                             str(mlcinfo).encode(), d.encode(),
+                             None if output_factor_file is None else str(output_factor_file).encode(),
+                             float(sid), default_medium.encode(), msg, len(msg))
+        if st != 0:
+            raise RuntimeError(f"reference set-up: {msg.value.decode()}")
+        self.nfields = int(self.get("nfields", np.int32)[0])
+
+    def get(self, name, dtype, field=-1):
+        L = lib()
+        n = L.ref_setup_get(name.encode(), field, None, 0)
+        if n < 0:
+            raise KeyError(name)
+        buf = np.zeros(n, np.uint8)
+        L.ref_setup_get(name.encode(), field, buf.ctypes.data, n)
+        return buf.view(dtype) if dtype is not None else buf.tobytes()
+
+    def field(self, f):
+        v = self.get("field", np.float32, f)
+        return dict(zip(self.FIELD, v))

@@ -8,7 +8,11 @@ against where the reference sources are absent.
 Needs the reference sources (oracle/refpin.REF_DIR) to build the harness.
 Stored: the inputs, then the reference's results -- howfar region, step and
 particle state, hownear distance; per stage the uniforms used, the particles
-pushed (sorted by stack, push order kept) and the escore calls."""
+pushed (sorted by stack, push order kept) and the escore calls.
+
+Also writes tests/golden/ref_setup.npz: the reference's host set-up (the
+egsphant, egsinp, mlcinfo and mlcinp readers and the per-field polygons of
+init.cu) on the plan files of tests/test_ref_setup.py."""
 import pathlib
 import sys
 
@@ -57,6 +61,24 @@ def main():
         out[key + "dreg"] = np.concatenate([ref["dreg"][i, :ref["dn"][i]] for i in range(n)])
         out[key + "de"] = np.concatenate([ref["de"][i, :ref["dn"][i]] for i in range(n)])
     path = HERE / "ref_pin_c3.npz"
+    np.savez_compressed(path, **out)
+    print(path, path.stat().st_size, "bytes")
+    setup_fixtures()
+
+
+def setup_fixtures():
+    """tests/golden/ref_setup.npz: the reference's host set-up (init.cu) on the
+    plan files of each case of tests/test_ref_setup.py."""
+    import tempfile
+    import test_ref_setup as TS
+    out = {}
+    for case in sorted(TS.CASES):
+        with tempfile.TemporaryDirectory() as d:
+            tmp = pathlib.Path(d)
+            _, c = TS.case_plan(tmp, case)
+            S = TS.run_reference(R, tmp, c)
+            out.update({f"{case}/{k}": v for k, v in TS.setup_arrays(S).items()})
+    path = HERE / "ref_setup.npz"
     np.savez_compressed(path, **out)
     print(path, path.stat().st_size, "bytes")
 

@@ -10,6 +10,7 @@ import subprocess
 import numpy as np
 import pytest
 
+from gegs_b200 import io_formats as F
 from gegs_b200 import physics_data as PD
 from gegs_b200 import workloads as W
 from gegs_b200.plan import load_plan
@@ -104,13 +105,13 @@ def test_cpp_dose_conversion_and_file_match_the_cli(plan_files, tmp_path):
     st, h, msg = _load(L, ini, phys)
     assert st == 0, msg
     nvox = int(L.gegs_plan_nvox(h))
-    mass = np.zeros(nvox)
+    mass = np.zeros(nvox, np.float32)
     assert L.gegs_plan_voxel_mass(h, mass.ctypes.data, nvox) == 0
     assert mass.tobytes() == plan.job.voxel_mass().tobytes()
     tally = np.random.default_rng(3).integers(0, 1 << 40, nvox).astype(np.int64)
     dose = np.zeros(nvox, np.float32)
     assert L.gegs_plan_dose(h, tally.ctypes.data, dose.ctypes.data, nvox) == 0
-    ref = (tally.astype(np.float64) * (2.0 ** -30) / plan.job.voxel_mass() * plan.dose_unit).astype(np.float32)
+    ref = F.dose_from_energy(tally.astype(np.float64) * (2.0 ** -30), plan.job.voxel_mass(), plan.dose_unit)
     assert dose.tobytes() == ref.tobytes()
     path = C.create_string_buffer(1024)
     assert L.gegs_plan_write_dose(h, dose.ctypes.data, nvox, path, len(path)) == 0
