@@ -25,6 +25,9 @@ def main():
     ap.add_argument("--timeline", action="store_true", help="persistent form with the wave timeline")
     ap.add_argument("--plan-histories", type=int, default=0, help="histories of the plan (fields split them; 0: --histories)")
     ap.add_argument("--first", type=int, default=0, help="first history of the run")
+    ap.add_argument("--max-waves", type=int, default=0,
+                    help="stop after this many waves (a short capture of the bulk waves; the run then reports "
+                         "the wave budget and its statistics cover those waves)")
     args = ap.parse_args()
     from . import build as B
     B.build()
@@ -38,7 +41,16 @@ def main():
     if args.timeline:
         print(json.dumps(timeline_summary(eng, args, dims)))
         return
-    st = eng.run(0, args.histories, mode=MODE_TIMED, batch=args.batch)
+    if args.max_waves:
+        from .engine import GegsError
+        try:
+            eng.run(0, args.histories, mode=MODE_TIMED, batch=args.batch, max_waves=args.max_waves)
+        except GegsError as err:
+            if err.status != 6:                         # GEGS_ERR_STEP_BUDGET: the waves ran out, as asked
+                raise
+        st = eng.stats()
+    else:
+        st = eng.run(0, args.histories, mode=MODE_TIMED, batch=args.batch)
     kinds = ["photon", "compton", "photo", "rayleigh", "pair", "electron", "moller", "brems", "bhabha", "annih",
              "source", "planner", "photon_jaws", "electron_jaws", "photon_mlc", "electron_mlc"]
     print(json.dumps({
