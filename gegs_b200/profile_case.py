@@ -44,13 +44,14 @@ def main():
     if args.max_waves:
         from .engine import GegsError
         try:
-            eng.run(0, args.histories, mode=MODE_TIMED, batch=args.batch, max_waves=args.max_waves)
+            eng.run(args.first, args.first + args.histories, mode=MODE_TIMED, batch=args.batch,
+                    max_waves=args.max_waves)
         except GegsError as err:
             if err.status != 6:                         # GEGS_ERR_STEP_BUDGET: the waves ran out, as asked
                 raise
         st = eng.stats()
     else:
-        st = eng.run(0, args.histories, mode=MODE_TIMED, batch=args.batch)
+        st = eng.run(args.first, args.first + args.histories, mode=MODE_TIMED, batch=args.batch)
     kinds = ["photon", "compton", "photo", "rayleigh", "pair", "electron", "moller", "brems", "bhabha", "annih",
              "source", "planner", "photon_jaws", "electron_jaws", "photon_mlc", "electron_mlc"]
     print(json.dumps({

@@ -126,7 +126,7 @@ def test_command_line_relative_dose_equals_c_statement(tmp_path, reldose):
     from gegs_b200.plan import load_plan
     from test_plan_io import _write_plan
 
-    job = W.config3(histories=5 * 40000, nphsp=3000, dims=(24, 24, 12))
+    job = W.config3(histories=5 * 200000, nphsp=3000, dims=(24, 24, 12))
     per_field = job.histories // len(job.fields)
     for norm_name, norm, array_name, array in (("Max", 1, "PTW1000", 2), ("Center", 2, "PTW729", 1)):
         d = tmp_path / norm_name
@@ -149,7 +149,7 @@ measured data = "meas.txt"
         name = run_plan(str(ini))
         dose = F.read_dose(name).reshape(-1)
         calc = PP.sample_plane(dose, p["x_bounds"], p["y_bounds"], p["z_bounds"], rp["start"], rp["sizes"], rp["dims"])
-        assert (calc > 0).sum() > 45                                  # the plane has dose
+        assert (calc > 0).sum() > 60                                  # the plane has dose
         rng = np.random.default_rng(norm)
         meas = calc * (1 + 0.05 * rng.standard_normal(calc.size)) + 0.02 * calc.max()
         (d / "data" / "meas.txt").write_text("".join(f"{float(v)!r}\n" for v in meas))
