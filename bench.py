@@ -94,8 +94,8 @@ class ClockSampler:
 
 def traffic_from_profile(kind):
     """DRAM bytes per transport step of the photon or electron kernels, from the
-    committed ncu summary ``profiles/transport_kernels_c3.md`` (all launches of
-    one run, DRAM read + write over the run's steps)."""
+    committed ncu summary ``profiles/transport_kernels_c3.md`` (three bulk waves
+    of the bench's step in the timed form, DRAM read + write over their steps)."""
     p = ROOT / "profiles" / "transport_kernels_c3.md"
     if not p.exists():
         return None
@@ -196,27 +196,37 @@ def c4_gradient(args, eng):
 def c5_batch(args, device):
     """C5 serving-style batch at its stated configuration: 32 independent plans
     (slab and CT head, 64^3 to 256x256x128 voxels, 1-7 fields, histories
-    log-uniform in 1e6..1e8), one engine, stream and persistent graph per plan.
-    Timed (host wall clock from the first launch to the last wait): all plans
-    concurrently and one by one with the default run options, then
-    concurrently with options from the autotuner (coordinate descent over
-    in-flight batch, grid, step budgets and refill threshold, timed on 2 % of
-    each plan's histories before the timed run)."""
+    log-uniform in 1e6..1e8), one engine per plan. Timed (host wall clock from
+    the first launch to the last wait) with the default run options: all plans
+    in one graph launch (a branch per plan), all plans launched one per stream,
+    and one plan after another; then in one graph launch with options from the
+    autotuner (coordinate descent over in-flight batch, grid, step budgets,
+    refill threshold and table staging, timed on a sample of each plan's
+    histories before the timed run)."""
     from gegs_b200 import workloads as W
     from gegs_b200.batch import PlanBatch
     jobs = W.config5(n_plans=args.c5_plans, hist_min=args.c5_hist_min, hist_max=args.c5_hist_max,
                      nphsp=1_000_000)
     total = sum(j.histories for j in jobs)
+    from gegs_b200.engine import launch_group
     pb = PlanBatch(jobs, device=device, memory_budget_gb=40.0)
     pb.run([max(1, j.histories // 100) for j in jobs])            # warm-up: graphs and queues
+    pb.run([max(1, j.histories // 100) for j in jobs], one_launch=False)
     t = time.perf_counter()
-    for e, j, o in zip(pb.engines, pb.jobs, pb.options):          # host cost of the launches alone
+    for e, j, o in zip(pb.engines, pb.jobs, pb.options):          # host cost of one launch per plan
         e.launch(0, 1, **o)
     launch_ms = (time.perf_counter() - t) * 1e3
     for e in pb.engines:
         e.wait()
-    pb.run()
+    t = time.perf_counter()
+    launch_group(pb.engines, [(0, 1)] * len(jobs), pb.options)    # host cost of the one group launch
+    group_launch_ms = (time.perf_counter() - t) * 1e3
+    for e in pb.engines:
+        e.wait()
+    pb.run()                                                       # all plans in one graph launch
     conc = pb.wall_s
+    pb.run(one_launch=False)                                       # one launch per plan, one stream each
+    conc_streams = pb.wall_s
     pb.run_sequential()
     seq = pb.wall_s
     pb.close()
@@ -234,7 +244,9 @@ def c5_batch(args, device):
                        f"histories log-uniform {args.c5_hist_min:.0e}..{args.c5_hist_max:.0e}",
            "histories": total, "concurrent_s": conc, "sequential_s": seq,
            "concurrent_histories_per_s": total / conc, "sequential_histories_per_s": total / seq,
-           "launch_ms_all_plans": launch_ms,
+           "concurrent": "all plans as one CUDA graph (one branch per plan), one launch (gegs_launch_group)",
+           "concurrent_streams_s": conc_streams,
+           "group_launch_ms": group_launch_ms, "launch_ms_all_plans": launch_ms,
            "autotuned": {"concurrent_s": tuned, "concurrent_histories_per_s": total / tuned, "tuning_s": tune_s,
                          "options": [{k: int(v) for k, v in o.items()} for o in tuned_opts]},
            "timing": "host wall clock from the first launch to the last wait"}

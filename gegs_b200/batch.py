@@ -17,7 +17,7 @@ import time
 
 import numpy as np
 
-from .engine import Engine
+from .engine import Engine, launch_group
 
 QUEUE_BYTES_PER_PARTICLE = 5.2e3      # event queues + electron step state per particle of `batch`
 
@@ -118,12 +118,19 @@ class PlanBatch:
             self.options.append(opts)
         self.wall_s = 0.0
 
-    def run(self, histories=None):
-        """Transport every plan's histories (or the first `histories[i]` of plan i) concurrently."""
+    def run(self, histories=None, one_launch=True):
+        """Transport every plan's histories (or the first `histories[i]` of plan i)
+        concurrently: with one_launch, as one graph with a branch per plan
+        (gegs_launch_group); otherwise one launch per plan, each on its engine's stream."""
         t = time.perf_counter()
-        for i, (e, j, o) in enumerate(zip(self.engines, self.jobs, self.options)):
+        ranges = [(0, j.histories if histories is None else histories[i]) for i, j in enumerate(self.jobs)]
+        for e in self.engines:
             e.reset_tally()
-            e.launch(0, j.histories if histories is None else histories[i], **o)
+        if one_launch:
+            launch_group(self.engines, ranges, self.options)
+        else:
+            for e, r, o in zip(self.engines, ranges, self.options):
+                e.launch(r[0], r[1], **o)
         stats = [e.wait() for e in self.engines]
         self.wall_s = time.perf_counter() - t
         return stats

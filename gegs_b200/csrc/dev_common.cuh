@@ -125,6 +125,7 @@ struct QueueSet {
     Part *buf[GX_NQ];
     uint32_t cap[GX_NQ];
     EStatePk *estate[GX_NESTATE];  // state of the electron continuation queues
+    uint32_t *peak;                // per queue the most records it held in one cycle (null: not recorded)
     uint32_t *count;      // [GX_NQ] items queued
     uint32_t *head;       // [GX_NQ] items taken by the running consumer
     uint32_t *done;       // [GX_NQ] finished blocks of the running consumer

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -34,6 +35,8 @@ constexpr unsigned long long estate_factor_sum()
 }
 
 }  // namespace
+
+static_assert(GX_NQ == GEGS_NQUEUES, "gegs_run_stats reports every queue");
 
 struct gegs_engine {
     int device = 0;
@@ -66,7 +69,7 @@ struct gegs_engine {
     TraceRec *d_trace = nullptr;
     uint32_t *d_trace_n = nullptr;
     uint32_t trace_cap = 0;
-    uint32_t *d_qmeta = nullptr;       // count[GX_NQ], head[GX_NQ], done[GX_NQ]
+    uint32_t *d_qmeta = nullptr;       // count[GX_NQ], head[GX_NQ], done[GX_NQ], peak[GX_NQ]
     Part *d_qbuf[GX_NQ] = {};
     EStatePk *d_estate[GX_NESTATE] = {};
     uint32_t qcap[GX_NQ] = {};
@@ -92,6 +95,7 @@ struct gegs_engine {
 
     gegs_run_stats last{};
     bool in_flight = false;            // gegs_launch queued a run that gegs_wait has not finished
+    std::shared_ptr<struct GroupRun> group;   // the group graph this engine's launched run belongs to
 
     // batch statistics (gegs_stat_*): per voxel the sum and sum of squares of
     // batch energies (MeV) and the tally at the last fold
@@ -183,8 +187,8 @@ gegs_status gegs_create(int device, gegs_engine **out)
     CK(cudaMalloc(&e->d_err, sizeof(uint32_t)), "err");
     CK(cudaMalloc(&e->d_stats, sizeof(unsigned long long) * 16), "stats");
     CK(cudaMalloc(&e->d_sched, sizeof(SchedState)), "sched");
-    CK(cudaMalloc(&e->d_qmeta, sizeof(uint32_t) * 3 * GX_NQ), "qmeta");
-    CK(cudaMemset(e->d_qmeta, 0, sizeof(uint32_t) * 3 * GX_NQ), "qmeta");
+    CK(cudaMalloc(&e->d_qmeta, sizeof(uint32_t) * 4 * GX_NQ), "qmeta");
+    CK(cudaMemset(e->d_qmeta, 0, sizeof(uint32_t) * 4 * GX_NQ), "qmeta");
     *out = e;
     return GEGS_OK;
 }
@@ -455,6 +459,7 @@ static void fill_queue_ctx(gegs_engine *e)
     Q.count = e->d_qmeta;
     Q.head = e->d_qmeta + GX_NQ;
     Q.done = e->d_qmeta + 2 * GX_NQ;
+    Q.peak = e->d_qmeta + 3 * GX_NQ;
     e->ctx.wave = &e->d_sched->waves;
     e->ctx.photon_done = &e->d_sched->photon_done;
     e->ctx.electron_done = &e->d_sched->electron_done;
@@ -511,14 +516,22 @@ static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
     join(3);
 }
 
-static gegs_status build_graph(gegs_engine *e, int grid, int threads)
+// Adds an engine's wave loop to g: a WHILE node whose body is one wave and
+// whose condition k_plan_cond sets on the device. With a planner, the loop is
+// preceded by the k_plan node that plans the first wave (a run launched on
+// its own launches k_plan before the graph instead).
+static gegs_status add_wave_loop(gegs_engine *e, cudaGraph_t g, int grid, int threads, bool with_planner)
 {
-    const int k = e->slot;
-    if (e->gexec[k] && e->graph_gen[k] == e->ctx_gen && e->graph_grid[k] == grid && e->graph_threads[k] == threads)
-        return GEGS_OK;
-    if (e->gexec[k]) { cudaGraphExecDestroy(e->gexec[k]); e->gexec[k] = nullptr; }
-    cudaGraph_t g;
-    CK(cudaGraphCreate(&g, 0), "graph create");
+    cudaGraphNode_t pnode = nullptr;
+    if (with_planner) {
+        void *args[] = {(void *)&e->ctx, (void *)&e->d_sched};
+        cudaKernelNodeParams kp = {};
+        kp.func = (void *)k_plan;
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(1);
+        kp.kernelParams = args;
+        CK(cudaGraphAddKernelNode(&pnode, g, nullptr, 0, &kp), "planner node");
+    }
     cudaGraphConditionalHandle handle;
     CK(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault), "conditional handle");
     cudaGraphNodeParams cp = {};
@@ -527,13 +540,26 @@ static gegs_status build_graph(gegs_engine *e, int grid, int threads)
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
     cudaGraphNode_t cnode;
-    CK(cudaGraphAddNode(&cnode, g, nullptr, 0, &cp), "conditional node");
+    CK(cudaGraphAddNode(&cnode, g, pnode ? &pnode : nullptr, pnode ? 1 : 0, &cp), "conditional node");
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     CK(cudaStreamBeginCaptureToGraph(e->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal), "capture");
     launch_wave_kernels(e, grid, threads);
     k_plan_cond<<<1, 1, 0, e->stream>>>(e->ctx, e->d_sched, handle);
     cudaGraph_t captured;
     CK(cudaStreamEndCapture(e->stream, &captured), "end capture");
+    return GEGS_OK;
+}
+
+static gegs_status build_graph(gegs_engine *e, int grid, int threads)
+{
+    const int k = e->slot;
+    if (e->gexec[k] && e->graph_gen[k] == e->ctx_gen && e->graph_grid[k] == grid && e->graph_threads[k] == threads)
+        return GEGS_OK;
+    if (e->gexec[k]) { cudaGraphExecDestroy(e->gexec[k]); e->gexec[k] = nullptr; }
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0), "graph create");
+    gegs_status st = add_wave_loop(e, g, grid, threads, false);
+    if (st != GEGS_OK) { cudaGraphDestroy(g); return st; }
     CK(cudaGraphInstantiate(&e->gexec[k], g, 0), "graph instantiate");
     cudaGraphDestroy(g);
     e->graph_gen[k] = e->ctx_gen;
@@ -542,17 +568,32 @@ static gegs_status build_graph(gegs_engine *e, int grid, int threads)
     return GEGS_OK;
 }
 
+// The executable graph of a group launch, shared by the group's engines and
+// destroyed when the last of them has waited for its run.
+struct GroupRun {
+    cudaGraphExec_t exec = nullptr;
+    ~GroupRun() { if (exec) cudaGraphExecDestroy(exec); }
+};
+
 static gegs_status run_finish(gegs_engine *e);
 
-// The transport of a run; with launch_only (persistent form) it returns once
-// the graph is queued on the engine's stream, and run_finish completes it.
-static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts,
-                            bool launch_only)
+// Everything a run needs before its kernels: options resolved into the
+// context, queues sized, the scheduler state and the counters reset on the
+// engine's stream.
+struct RunSetup {
+    gegs_run_opts o;
+    int grid, threads;
+    uint32_t max_waves;
+};
+
+static gegs_status prepare_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts,
+                               RunSetup &R)
 {
     if (!e || !e->have_scene || hist_end < hist_begin) return GEGS_ERR_ARG;
     if (e->in_flight) { e->err = "a launched run has not been waited for (gegs_wait)"; return GEGS_ERR_ARG; }
     CK(cudaSetDevice(e->device), "cudaSetDevice");
-    gegs_run_opts o = {};
+    gegs_run_opts &o = R.o;
+    o = {};
     if (opts) o = *opts;
     uint32_t batch = o.batch ? o.batch : default_batch(e, hist_end - hist_begin);
     int threads = o.threads_per_block ? o.threads_per_block : 256;
@@ -581,7 +622,7 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
     hs.max_waves = max_waves;
     hs.refill_below = o.refill_below ? o.refill_below : (batch / 4u > 0u ? batch / 4u : 1u);
     CK(cudaMemcpyAsync(e->d_sched, &hs, sizeof hs, cudaMemcpyHostToDevice, e->stream), "sched H2D");
-    CK(cudaMemsetAsync(e->d_qmeta, 0, sizeof(uint32_t) * 3 * GX_NQ, e->stream), "qmeta reset");
+    CK(cudaMemsetAsync(e->d_qmeta, 0, sizeof(uint32_t) * 4 * GX_NQ, e->stream), "qmeta reset");
     CK(cudaMemsetAsync(e->d_err, 0, sizeof(uint32_t), e->stream), "err reset");
     CK(cudaMemsetAsync(e->d_stats, 0, sizeof(unsigned long long) * 16, e->stream), "stats reset");
     if (e->d_timeline) {
@@ -595,6 +636,23 @@ static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_e
                            cudaMemcpyHostToDevice, e->stream), "timeline reset");
     }
 
+    R.grid = grid;
+    R.threads = threads;
+    R.max_waves = max_waves;
+    return GEGS_OK;
+}
+
+// The transport of a run; with launch_only (persistent form) it returns once
+// the graph is queued on the engine's stream, and run_finish completes it.
+static gegs_status run_impl(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts,
+                            bool launch_only)
+{
+    RunSetup R;
+    gegs_status st = prepare_run(e, hist_begin, hist_end, opts, R);
+    if (st != GEGS_OK) return st;
+    const gegs_run_opts &o = R.o;
+    const int grid = R.grid, threads = R.threads;
+    const uint32_t max_waves = R.max_waves;
     for (int k = 0; k < 16; k++) { e->last.stage_ms[k] = 0.0; e->last.stage_launches[k] = 0; }
     if (o.mode == GEGS_MODE_PERSISTENT) {
         st = build_graph(e, grid, threads);
@@ -739,6 +797,7 @@ static gegs_status run_finish(gegs_engine *e)
 {
     e->in_flight = false;
     CK(cudaStreamSynchronize(e->stream), "run sync");
+    e->group.reset();
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e->ev0, e->ev1);
     uint32_t errbits = 0;
@@ -747,6 +806,9 @@ static gegs_status run_finish(gegs_engine *e)
     CK(cudaMemcpy(&errbits, e->d_err, sizeof errbits, cudaMemcpyDeviceToHost), "err D2H");
     CK(cudaMemcpy(stats, e->d_stats, sizeof stats, cudaMemcpyDeviceToHost), "stats D2H");
     CK(cudaMemcpy(&hsr, e->d_sched, sizeof hsr, cudaMemcpyDeviceToHost), "sched D2H");
+    CK(cudaMemcpy(e->last.queue_peak, e->d_qmeta + 3 * GX_NQ, sizeof(uint32_t) * GX_NQ, cudaMemcpyDeviceToHost),
+       "queue peaks D2H");
+    for (int q = 0; q < GX_NQ; q++) e->last.queue_cap[q] = e->qcap[q];
     return finish_stats(e, errbits, stats, hsr.waves, ms);
 }
 
@@ -769,6 +831,56 @@ extern "C" gegs_status gegs_wait(gegs_engine *e)
     if (!e->in_flight) { e->err = "gegs_wait: no launched run"; return GEGS_ERR_ARG; }
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     return run_finish(e);
+}
+
+extern "C" gegs_status gegs_launch_group(gegs_engine *const *engines, int32_t n, const uint64_t *hist_begin,
+                                         const uint64_t *hist_end, const gegs_run_opts *opts)
+{
+    if (!engines || n < 1 || !hist_begin || !hist_end) return GEGS_ERR_ARG;
+    for (int i = 0; i < n; i++) {
+        if (!engines[i]) return GEGS_ERR_ARG;
+        if (engines[i]->device != engines[0]->device) {
+            engines[i]->err = "gegs_launch_group: the engines are on different devices";
+            return GEGS_ERR_ARG;
+        }
+        for (int j = 0; j < i; j++)
+            if (engines[j] == engines[i]) { engines[i]->err = "gegs_launch_group: an engine appears twice"; return GEGS_ERR_ARG; }
+    }
+    std::vector<RunSetup> R(n);
+    for (int i = 0; i < n; i++) {
+        gegs_run_opts o = {};
+        if (opts) o = opts[i];
+        o.mode = GEGS_MODE_PERSISTENT;
+        gegs_status st = prepare_run(engines[i], hist_begin[i], hist_end[i], &o, R[i]);
+        if (st != GEGS_OK) return st;
+    }
+    gegs_engine *e = engines[0];          // errors are reported on the first engine
+    cudaGraph_t g;
+    CK(cudaGraphCreate(&g, 0), "graph create");
+    for (int i = 0; i < n; i++) {
+        gegs_status st = add_wave_loop(engines[i], g, R[i].grid, R[i].threads, true);
+        if (st != GEGS_OK) { cudaGraphDestroy(g); if (engines[i] != e) e->err = engines[i]->err; return st; }
+    }
+    auto grp = std::make_shared<GroupRun>();
+    cudaError_t ce = cudaGraphInstantiate(&grp->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) { e->err = std::string("group graph instantiate: ") + cudaGetErrorString(ce); return GEGS_ERR_CUDA; }
+    // the group runs on the first engine's stream once every engine's set-up is done
+    cudaStream_t s = e->stream;
+    for (int i = 1; i < n; i++) {
+        CK(cudaEventRecord(engines[i]->ev_fork, engines[i]->stream), "event");
+        CK(cudaStreamWaitEvent(s, engines[i]->ev_fork, 0), "stream wait");
+    }
+    for (int i = 0; i < n; i++) CK(cudaEventRecord(engines[i]->ev0, s), "event");
+    CK(cudaGraphLaunch(grp->exec, s), "group graph launch");
+    for (int i = 0; i < n; i++) {
+        CK(cudaEventRecord(engines[i]->ev1, s), "event");
+        if (i > 0) CK(cudaStreamWaitEvent(engines[i]->stream, engines[i]->ev1, 0), "stream wait");
+        for (int k = 0; k < 16; k++) { engines[i]->last.stage_ms[k] = 0.0; engines[i]->last.stage_launches[k] = 0; }
+        engines[i]->group = grp;
+        engines[i]->in_flight = true;
+    }
+    return GEGS_OK;
 }
 
 extern "C" gegs_status gegs_get_tally(gegs_engine *e, int64_t *out, uint64_t nvox)
@@ -1011,6 +1123,7 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
     c.q.count = qmeta;
     c.q.head = qmeta + GX_NQ;
     c.q.done = qmeta + 2 * GX_NQ;
+    c.q.peak = nullptr;
     c.err = err;
     c.stats = stats;
     c.wave = &sched->waves;

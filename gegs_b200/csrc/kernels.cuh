@@ -54,6 +54,10 @@ __device__ __forceinline__ void consumer_done(const DevCtx &C, int q, int q2 = -
         __threadfence();
         uint32_t prev = atomicAdd(&C.q.done[q], 1u);
         if (prev == gridDim.x - 1) {
+            if (C.q.peak) {
+                atomicMax(&C.q.peak[q], *((volatile uint32_t *)&C.q.count[q]));
+                if (q2 >= 0) atomicMax(&C.q.peak[q2], *((volatile uint32_t *)&C.q.count[q2]));
+            }
             C.q.count[q] = 0;
             C.q.head[q] = 0;
             C.q.done[q] = 0;

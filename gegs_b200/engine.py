@@ -20,7 +20,7 @@ MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 
 EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_set_timeline", "gegs_get_timeline", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
            "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_set_tally", "gegs_get_dose", "gegs_get_stats",
-           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version",
+           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_launch_group", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version",
            "gegs_check_physics", "gegs_stat_begin", "gegs_stat_fold", "gegs_stat_get"]
 
 
@@ -46,7 +46,8 @@ class RunStats(C.Structure):
     _fields_ = [("processed", C.c_uint64 * 10), ("photon_steps", C.c_uint64), ("electron_steps", C.c_uint64),
                 ("waves", C.c_uint32), ("error_bits", C.c_uint32), ("device_ms", C.c_double),
                 ("stage_ms", C.c_double * 16), ("stage_launches", C.c_uint64 * 16),
-                ("photon_steps_class", C.c_uint64 * 3), ("electron_steps_class", C.c_uint64 * 3)]
+                ("photon_steps_class", C.c_uint64 * 3), ("electron_steps_class", C.c_uint64 * 3),
+                ("queue_peak", C.c_uint32 * 25), ("queue_cap", C.c_uint32 * 25)]
 
 
 _lib = None
@@ -71,6 +72,7 @@ def load_library(path=None):
     L.gegs_run_noalloc.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint32]
     L.gegs_launch.argtypes = [vp, C.c_uint64, C.c_uint64, C.POINTER(RunOpts)]
     L.gegs_wait.argtypes = [vp]
+    L.gegs_launch_group.argtypes = [vp, C.c_int32, vp, vp, vp]
     L.gegs_set_beamlet_weights.argtypes = [vp, vp, C.c_uint32]
     L.gegs_backward.argtypes = [vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint32, C.POINTER(RunOpts)]
     L.gegs_reset_tally.argtypes = [vp]
@@ -185,6 +187,13 @@ class Engine:
         self._check(self.L.gegs_wait(self.h))
         return self.stats()
 
+    @staticmethod
+    def _opts(o):
+        return RunOpts(MODE_PERSISTENT, o.get("batch", 0), o.get("blocks_per_sm", 0), o.get("threads", 0), 0,
+                       (o.get("photon_budget", 0) & 0xFFFF) | (o.get("electron_budget", 0) << 16),
+                       o.get("refill_below", 0), 0, RUN_STAGE_TABLES if o.get("stage_tables") else 0)
+
+
     def reset_tally(self):
         self._check(self.L.gegs_reset_tally(self.h))
 
@@ -260,7 +269,8 @@ class Engine:
         return dict(processed=list(s.processed), photon_steps=s.photon_steps, electron_steps=s.electron_steps,
                     waves=s.waves, error_bits=s.error_bits, device_ms=s.device_ms,
                     stage_ms=list(s.stage_ms), stage_launches=list(s.stage_launches),
-                    photon_steps_class=list(s.photon_steps_class), electron_steps_class=list(s.electron_steps_class))
+                    photon_steps_class=list(s.photon_steps_class), electron_steps_class=list(s.electron_steps_class),
+                    queue_peak=list(s.queue_peak), queue_cap=list(s.queue_cap))
 
     def set_trace(self, capacity: int):
         self._check(self.L.gegs_set_trace(self.h, capacity))
@@ -276,3 +286,18 @@ class Engine:
         p = C.c_void_p()
         self._check(self.L.gegs_tally_device_ptr(self.h, C.byref(p)))
         return p.value
+
+
+def launch_group(engines, ranges, options=None):
+    """Queue the persistent-form runs of several engines (one device) as one
+    graph launch (gegs_launch_group); ranges[i] = (h0, h1) of engine i and
+    options[i] its run options as for Engine.launch. Finish each with wait()."""
+    n = len(engines)
+    if n == 0 or len(ranges) != n or (options is not None and len(options) != n):
+        raise ValueError("one range (and one option set) per engine")
+    L = engines[0].L
+    handles = (C.c_void_p * n)(*[e.h for e in engines])
+    h0 = (C.c_uint64 * n)(*[int(r[0]) for r in ranges])
+    h1 = (C.c_uint64 * n)(*[int(r[1]) for r in ranges])
+    opts = (RunOpts * n)(*[Engine._opts(o) for o in (options or [{}] * n)])
+    engines[0]._check(L.gegs_launch_group(handles, n, h0, h1, opts))

@@ -76,6 +76,8 @@ typedef struct gegs_run_opts {
 
 #define GEGS_RUN_STAGE_TABLES 1u
 
+#define GEGS_NQUEUES 25
+
 typedef struct gegs_run_stats {
     uint64_t processed[10];    /* particles handled per stage: photon, compton, photo, rayleigh,
                                   pair, electron, moller, brems, bhabha, annih */
@@ -89,6 +91,11 @@ typedef struct gegs_run_stats {
     uint64_t stage_launches[16];
     uint64_t photon_steps_class[3];   /* steps in the jaws, the MLC, the phantom (persistent and timed forms) */
     uint64_t electron_steps_class[3];
+    /* per event queue (10 stages, 12 continuation queues, 2 near-boundary
+     * queues, 1 long-track queue): the most records it held in one cycle of
+     * the persistent and timed forms, and its capacity (0 after gegs_run_noalloc) */
+    uint32_t queue_peak[GEGS_NQUEUES];
+    uint32_t queue_cap[GEGS_NQUEUES];
 } gegs_run_stats;
 
 /* Engine life cycle */
@@ -126,6 +133,15 @@ gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, con
  * the device. One launched run per engine at a time. */
 gegs_status gegs_launch(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts);
 gegs_status gegs_wait(gegs_engine *e);
+
+/* Several plans in one launch: the persistent-form runs of n engines on one
+ * device (engine i transports [hist_begin[i], hist_end[i]) with opts[i]; opts
+ * may be NULL) as one CUDA graph, one branch per engine -- its planner, then
+ * its wave loop -- launched once on the first engine's stream. Each engine is
+ * then finished with gegs_wait; its device_ms is the time of the whole group.
+ * The reference runs plans and fields one after another (CUDA_EGS.cu:1715-1742). */
+gegs_status gegs_launch_group(gegs_engine *const *engines, int32_t n, const uint64_t *hist_begin,
+                              const uint64_t *hist_end, const gegs_run_opts *opts);
 
 /* No counterpart in the reference: an addition of this library.
  *

@@ -44,3 +44,14 @@ def test_create_without_gpu_reports_error_not_crash():
         assert err.status == 2
     else:
         raise AssertionError("engine creation must fail loudly without a GPU")
+
+
+def test_engine_binding_has_every_method():
+    """The Python binding exposes each C entry point a caller needs as an
+    Engine method (checked without a GPU)."""
+    from gegs_b200.engine import Engine, launch_group
+    for m in ("set_physics", "set_scene", "run", "launch", "wait", "stats", "tally", "reset_tally", "dose",
+              "set_tally", "checkpoint", "resume", "set_timeline", "timeline", "set_trace", "get_trace",
+              "stat_begin", "stat_fold", "stat_get", "backward", "set_beamlet_weights", "set_phsp"):
+        assert callable(getattr(Engine, m, None)), m
+    assert callable(launch_group)

@@ -33,6 +33,46 @@ def test_concurrent_plans_match_their_own_runs(oracle):
     pb.close()
 
 
+def test_launch_group_checks_its_arguments():
+    from gegs_b200.engine import launch_group
+    with pytest.raises(ValueError):
+        launch_group([], [])
+    with pytest.raises(ValueError):
+        launch_group([object()], [(0, 1), (1, 2)])
+
+
+@pytest.mark.gpu
+def test_one_launch_equals_launches_per_plan_and_the_oracle(oracle):
+    """All plans as one graph launch (a branch per plan, gegs_launch_group):
+    each plan's tally equals its launch on its own stream and the oracle; the
+    group refuses an engine twice and an engine with a run in flight."""
+    from gegs_b200.batch import PlanBatch
+    from gegs_b200.engine import GegsError, launch_group
+    jobs = W.config5(n_plans=5, hist_min=2000, hist_max=20000, nphsp=5000, dims_max=(48, 48, 32), dims_min=24)
+    pb = PlanBatch(jobs, memory_budget_gb=4.0)
+    st = pb.run(one_launch=True)
+    one = pb.tallies()
+    pb.run(one_launch=False)
+    per = pb.tallies()
+    for a, b, s in zip(one, per, st):
+        np.testing.assert_array_equal(a, b)
+        assert s["error_bits"] == 0 and a.sum() > 0 and s["waves"] > 0
+    for k in (0, 3):
+        ref, _ = oracle.run(jobs[k].physics, jobs[k].scene(), 0, jobs[k].histories)
+        np.testing.assert_array_equal(one[k], ref)
+    e = pb.engines
+    with pytest.raises(GegsError):
+        launch_group([e[0], e[1], e[0]], [(0, 10)] * 3)
+    e[2].launch(0, 10)
+    with pytest.raises(GegsError):
+        launch_group([e[1], e[2]], [(0, 10)] * 2)
+    e[2].wait()
+    launch_group(e[:2], [(0, 100), (0, 100)])                       # the engines are usable again
+    for x in e[:2]:
+        x.wait()
+    pb.close()
+
+
 @pytest.mark.gpu
 def test_autotuned_plans_keep_their_tallies(oracle):
     """The autotuner changes only how a plan runs (batch, grid, step budgets,
