@@ -490,11 +490,15 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e = H * args.steps * world / (float(tt[0]) / 1e3)
 
+    # Every rank leaves the process group here, so that no rank waits on a
+    # collective while rank 0 alone measures the rest (at N > 1 only the
+    # roofline; the CPU baseline, sigma, plain form, C4 and C5 at N = 1).
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
     if rank != 0:
-        if dist is not None:
-            dist.barrier()
-            dist.destroy_process_group()
         return
+    extras = world == 1
 
     # ---- roofline of the dominant kernel (timed mode, outside the timed region)
     eng.set_phsp(job.phsp)
@@ -522,11 +526,11 @@ def main():
     share = {k: float(ms[i] / total_ms) for i, k in enumerate(kinds) if i != 11}
 
     # ---- statistical uncertainty -> time to 1 % (outside the timed region) --
-    sigma = sigma_series(eng, job, args, ropt, value) if args.sigma_batches >= 2 else None
+    sigma = sigma_series(eng, job, args, ropt, value) if extras and args.sigma_batches >= 2 else None
 
     # ---- the plain form at the reference's launch shape, same histories ------
     plain = None
-    if args.plain_histories > 0:
+    if extras and args.plain_histories > 0:
         hp = args.plain_histories
         pst = eng.run(0, hp, mode=MODE_PLAIN, batch=480_000, blocks_per_sm=5, threads=128)
         qst = eng.run(0, hp, **dict(ropt, mode=MODE_PERSISTENT))
@@ -538,13 +542,13 @@ def main():
                          "and gamma; the ratio is the time-to-1% ratio"}
 
     # ---- C4: beamlet gradient by replay vs forward and finite differences ---
-    grad = c4_gradient(args, eng) if args.c4_histories > 0 else None
+    grad = c4_gradient(args, eng) if extras and args.c4_histories > 0 else None
     nvox = eng.nvox
-    eng.close()                                    # its event queues (up to ~87 GB) before the C5 engines
-    batched = c5_batch(args, local) if args.c5_plans > 0 else None
+    eng.close()                                    # its event queues (up to ~120 GB) before the C5 engines
+    batched = c5_batch(args, local) if extras and args.c5_plans > 0 else None
 
     cpu = None
-    if not args.no_cpu:
+    if extras and not args.no_cpu:
         crate, cn, cdt, cores = cpu_histories_per_s(job, seconds=args.cpu_seconds)
         r1, n1, dt1, _ = cpu_histories_per_s(job, seconds=3.0, threads=1)
         cpu = {"value": crate, "unit": "histories/s", "cores": cores, "kind": "port",
@@ -582,9 +586,6 @@ def main():
         "wall_s": wall,
     }
     print(json.dumps(line))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -12,6 +12,7 @@
 // back after every launch (CUDA_EGS.cu:226-365, 498-799).
 #pragma once
 #include "dev_electron.cuh"
+#include "../../include/gegs.h"     // gegs_probe_state
 
 // steps one particle may take inside one consumer launch before it is dropped
 // and GX_ERR_STEP_BUDGET is raised (guards the persistent loops against a
@@ -524,6 +525,37 @@ __global__ void k_plan_cond(const __grid_constant__ DevCtx C, SchedState *st, cu
 {
     uint32_t pending = plan_wave(C, st);
     cudaGraphSetConditional(handle, pending);
+}
+
+// ---- geometry probe (gegs_probe_geometry) ----------------------------------
+__device__ __forceinline__ Part probe_part(const gegs_probe_state &s)
+{
+    Part p = {};
+    p.region = s.region; p.charge = s.charge; p.leafIndex = s.leafIndex; p.bank = s.bank;
+    p.module = s.module; p.field = s.field; p.status = s.status;
+    p.wt = s.wt; p.e = s.e; p.x = s.x; p.y = s.y; p.z = s.z; p.u = s.u; p.v = s.v; p.w = s.w;
+    return p;
+}
+
+__global__ void k_probe_geometry(const __grid_constant__ DevCtx C, uint32_t n, const gegs_probe_state *in,
+                                 const float *t_in, uint32_t *far_region, float *far_t, gegs_probe_state *far_out,
+                                 float *near_t)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const gegs_probe_state s = in[i];
+    Part p = probe_part(s);
+    float t = t_in[i];
+    bool ok;
+    far_region[i] = howfar(C, p, t, ok);
+    far_t[i] = t;
+    gegs_probe_state o = s;
+    o.leafIndex = p.leafIndex; o.bank = p.bank; o.module = p.module;
+    far_out[i] = o;
+    Part q = probe_part(s);
+    float tp = 0.0f;
+    hownear(C, q, tp, ok);
+    near_t[i] = tp;
 }
 
 __global__ void k_dose(const unsigned long long *tally, const float *mass, double unit, double *out, uint64_t n)

@@ -20,7 +20,7 @@ MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 
 EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_set_timeline", "gegs_get_timeline", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
            "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_set_tally", "gegs_get_dose", "gegs_get_stats",
-           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_launch_group", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version",
+           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_launch_group", "gegs_probe_geometry", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version",
            "gegs_check_physics", "gegs_stat_begin", "gegs_stat_fold", "gegs_stat_get"]
 
 
@@ -40,6 +40,13 @@ class RunOpts(C.Structure):
                 ("refill_below", C.c_uint32), ("queue_cap", C.c_uint32), ("flags", C.c_uint32)]
 
 RUN_STAGE_TABLES = 1
+
+
+# gegs_probe_state (include/gegs.h)
+PROBE_DTYPE = np.dtype([("region", "<u4"), ("charge", "i1"), ("leafIndex", "i1"), ("bank", "i1"), ("module", "u1"),
+                        ("field", "u1"), ("status", "u1"), ("pad0", "u1"), ("pad1", "u1"),
+                        ("wt", "<f4"), ("e", "<f4"), ("x", "<f4"), ("y", "<f4"), ("z", "<f4"),
+                        ("u", "<f4"), ("v", "<f4"), ("w", "<f4"), ("dnear", "<f4"), ("hist", "<u4"), ("pad2", "<u4")])
 
 
 class RunStats(C.Structure):
@@ -73,6 +80,7 @@ def load_library(path=None):
     L.gegs_launch.argtypes = [vp, C.c_uint64, C.c_uint64, C.POINTER(RunOpts)]
     L.gegs_wait.argtypes = [vp]
     L.gegs_launch_group.argtypes = [vp, C.c_int32, vp, vp, vp]
+    L.gegs_probe_geometry.argtypes = [vp, C.c_uint32, vp, vp, vp, vp, vp, vp]
     L.gegs_set_beamlet_weights.argtypes = [vp, vp, C.c_uint32]
     L.gegs_backward.argtypes = [vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint32, C.POINTER(RunOpts)]
     L.gegs_reset_tally.argtypes = [vp]
@@ -186,6 +194,21 @@ class Engine:
     def wait(self):
         self._check(self.L.gegs_wait(self.h))
         return self.stats()
+
+    def probe_geometry(self, states, t_in):
+        """howfar (step t_in) and hownear of each state on the device
+        (gegs_probe_geometry): region entered, step, state after howfar, and
+        the distance to the nearest boundary."""
+        s = np.ascontiguousarray(states, PROBE_DTYPE)
+        t = np.ascontiguousarray(t_in, np.float32)
+        n = len(s)
+        reg = np.zeros(n, np.uint32)
+        ft = np.zeros(n, np.float32)
+        out = np.zeros(n, PROBE_DTYPE)
+        near = np.zeros(n, np.float32)
+        self._check(self.L.gegs_probe_geometry(self.h, n, s.ctypes.data, t.ctypes.data, reg.ctypes.data,
+                                               ft.ctypes.data, out.ctypes.data, near.ctypes.data))
+        return dict(region=reg, t=ft, particle=out, tperp=near)
 
     @staticmethod
     def _opts(o):

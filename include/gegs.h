@@ -54,9 +54,9 @@ typedef enum gegs_mode {
 
 typedef struct gegs_run_opts {
     int32_t mode;              /* gegs_mode */
-    uint32_t batch;            /* particles kept in flight (0 = a power of two near half the run's histories,
-                                  64K to 16M, within 60 % of free device memory; queue memory ~5.2 KB each,
-                                  ~87 GB at 16M) */
+    uint32_t batch;            /* particles kept in flight (0 = 60 % of the run's histories in steps of 64K,
+                                  64K to 24M, within 70 % of free device memory; queue memory ~5 KB each,
+                                  ~120 GB at 24M) */
     int32_t blocks_per_sm;     /* 0 = default (6: grid = 6 x SM count) */
     int32_t threads_per_block; /* 0 = default */
     uint32_t max_waves;        /* safety budget (0 = default) */
@@ -213,6 +213,25 @@ gegs_status gegs_get_stats(gegs_engine *e, gegs_run_stats *out);
 gegs_status gegs_stat_begin(gegs_engine *e);
 gegs_status gegs_stat_fold(gegs_engine *e);
 gegs_status gegs_stat_get(gegs_engine *e, double *mean, double *rel_se, uint64_t nvox, uint32_t *nbatch);
+
+/* A particle state for gegs_probe_geometry (56 bytes). */
+typedef struct gegs_probe_state {
+    uint32_t region;
+    int8_t charge, leafIndex, bank;
+    uint8_t module, field, status, pad0, pad1;
+    float wt, e, x, y, z, u, v, w, dnear;
+    uint32_t hist, pad2;
+} gegs_probe_state;
+
+/* The device's geometry routines on n given states, for checking them against
+ * other implementations (no counterpart in the reference): per state i, howfar
+ * of the step t_in[i] gives the region entered far_region[i], the step
+ * far_t[i] and the state after the call far_out[i] (its leaf index, bank and
+ * module may change); hownear of the unchanged state gives near_t[i]. The
+ * routines are the transport's own (geom.cu:54-1543 restated). Needs a scene;
+ * allocates device memory for the call. */
+gegs_status gegs_probe_geometry(gegs_engine *e, uint32_t n, const gegs_probe_state *in, const float *t_in,
+                                uint32_t *far_region, float *far_t, gegs_probe_state *far_out, float *near_t);
 
 /* Device pointer of the tally (for callers that keep results in HBM). */
 gegs_status gegs_tally_device_ptr(gegs_engine *e, void **out);

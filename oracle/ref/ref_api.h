@@ -22,6 +22,8 @@ int ref_setup_run(const char *egsphant, const char *mlc_egsinp, const char *jaws
                   const char *data_directory, const char *outfac_file, float sid, const char *default_medium,
                   char *msg, size_t msg_len);
 long ref_setup_get(const char *name, int field, void *dst, size_t bytes);
+/* a whole transport of histories [h0, h1) of the loaded scene by the reference's kernels */
+long ref_transport(uint64_t h0, uint64_t h1, uint64_t seed, double *tally, uint64_t nvox);
 #ifdef __cplusplus
 }
 #endif

@@ -54,12 +54,18 @@ ref_uniform_stream g_ref_uniforms;
 
 #include "ref_math.h"
 
-// ---- escore (scoring.cu:14-26) as a recorder of every call ----------------
+// ---- escore (scoring.cu:14-26) as a recorder of every call, or, during a
+// whole transport (ref_transport), the reference's own sum per phantom voxel
 struct ref_deposit { uint32_t region; float energy; };
 static std::vector<ref_deposit> g_deposits;
+static double *g_transport_tally = nullptr;
 
 __device__ void escore(uint region, float energy)
 {
+    if (g_transport_tally) {
+        if (region >= vac_and_oth) g_transport_tally[region - vac_and_oth] += (double)energy;
+        return;
+    }
     g_deposits.push_back(ref_deposit{region, energy});
 }
 
@@ -88,6 +94,8 @@ static std::vector<uint> g_tab_i_array;
 static std::vector<region_data_t> g_regions;
 static std::vector<float> g_xb, g_yb, g_zb;
 static std::vector<gegs_field> g_fields;
+static const gegs_phsp_record *g_phsp = nullptr;   // the caller's scene keeps it alive
+static uint64_t g_nphsp = 0;
 static curandState g_state;
 static std::vector<particle_t> g_stack_mem[NUM_SIMU_CAT];
 static const int kStackCap = 4096;
@@ -221,6 +229,9 @@ extern "C" int ref_load(const gegs_physics *P, const gegs_scene *S)
         boundaryYZ[i] = make_float2(S->boundaryYZ[i][0], S->boundaryYZ[i][1]);
     }
     g_fields.assign(S->fields, S->fields + S->nfields);
+    g_phsp = S->phsp;
+    g_nphsp = S->nphsp;
+    z_phsp = S->z_phsp;
 
     // ---- stacks and the random-number state
     devStates = &g_state;
@@ -586,4 +597,72 @@ extern "C" long ref_setup_get(const char *name, int f, void *dst, size_t bytes)
     else return -1;
     if (dst) std::memcpy(dst, src, size < bytes ? size : bytes);
     return (long)size;
+}
+
+
+// ---------------------------------------------------------------------------
+// A whole transport by the reference's own kernels: histories [h0, h1) of the
+// loaded scene, field by field. Each batch of primaries goes onto the photon
+// stack as load_stack_from_phspfile puts them there (CUDA_EGS.cu:54-136), and
+// the ten stage kernels run, each draining its stack, until every stack is
+// empty. The random numbers come from a seeded generator (shim/curand_kernel.h),
+// so the result is an independent sample of the reference's transport, for
+// statistical comparison with the package's dose. tally: energy per voxel in
+// MeV, added to. Returns the number of stack overflows seen (0 expected).
+// ---------------------------------------------------------------------------
+extern "C" long ref_transport(uint64_t h0, uint64_t h1, uint64_t seed, double *tally, uint64_t nvox)
+{
+    if (!g_phsp || g_nphsp == 0 || !tally || nvox != (uint64_t)size_phantom) return -1;
+    const int kBatch = 256;
+    long overflows = 0;
+    g_transport_tally = tally;
+    g_ref_uniforms = ref_uniform_stream{nullptr, 0u, 0u, 0u, 1, seed * 0x2545F4914F6CDD1Dull + 1u};
+    for (int f = 0; f < (int)g_fields.size(); f++) {
+        const gegs_field &F = g_fields[(size_t)f];
+        const uint64_t a = std::max<uint64_t>(h0, F.hist_begin), b = std::min<uint64_t>(h1, F.hist_end);
+        if (a >= b) continue;
+        ref_select_field(f);
+        g_field = f;
+        for (uint64_t h = a; h < b; h += kBatch) {
+            const uint64_t e = std::min<uint64_t>(b, h + kBatch);
+            for (uint64_t k = h; k < e; k++) {
+                const gegs_phsp_record &r = g_phsp[((k - F.hist_begin) / (uint64_t)(F.nrepeat + 1)) % g_nphsp];
+                particle_t p;
+                std::memset(&p, 0, sizeof p);
+                char q = (r.latch & 0x40000000u) ? -1 : ((r.latch & 0x20000000u) ? 1 : 0);
+                float w = std::sqrt(1 - r.u * r.u - r.v * r.v);
+                float wt = r.wt;
+                if (wt < 0) { w = -w; wt = -wt; }
+                p.status = q == 0 ? p_new_particle : e_new_particle;
+                p.nRepeat = 0;
+                p.charge = q;
+                p.process = 1;
+                p.e = r.e < 0 ? -r.e : r.e;
+                p.wt = wt;
+                p.region = 0;
+                p.leafIndex = INIT_MLC_STAT;
+                p.bank = -1;
+                p.module = module_order[m_FirstMd];
+                p.latch = 0;
+                p.x = r.x; p.y = r.y; p.z = z_phsp;
+                p.u = r.u; p.v = r.v; p.w = w;
+                p.dnear = INFI_DIST;
+                stack[p_photon_step][++np[p_photon_step]] = p;
+            }
+            bool busy = true;
+            while (busy) {
+                busy = false;
+                for (int s = 0; s < NUM_SIMU_CAT; s++) {
+                    if (np[s] < 0) continue;
+                    run_kernel(s);
+                    busy = true;
+                    for (int q2 = 0; q2 < NUM_SIMU_CAT; q2++)
+                        if (np[q2] >= np_max[q2] - 1) overflows++;
+                }
+            }
+        }
+    }
+    g_transport_tally = nullptr;
+    g_ref_uniforms = ref_uniform_stream{nullptr, 0u, 0u, 0u, 0, 0ull};
+    return overflows;
 }

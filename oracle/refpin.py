@@ -73,6 +73,8 @@ def lib():
         L.ref_setup_run.argtypes = [C.c_char_p] * 6 + [C.c_float, C.c_char_p, C.c_char_p, C.c_size_t]
         L.ref_setup_get.argtypes = [C.c_char_p, C.c_int, vp, C.c_size_t]
         L.ref_setup_get.restype = C.c_long
+        L.ref_transport.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, vp, C.c_uint64]
+        L.ref_transport.restype = C.c_long
         _lib = L
     return _lib
 
@@ -186,6 +188,19 @@ class Pair(OraclePair):
         c = np.array([cs[0], cs[1], 0.0, 0.0], np.float32)
         lib().ref_probe_uphi(which, a, b, p.ctypes.data, c.ctypes.data, u)
         return (po, co), (p[0], c)
+
+    def transport(self, h0, h1, seed=1):
+        """Histories [h0, h1) transported by the reference's own kernels (one
+        CPU thread, a seeded generator for the random numbers): energy per
+        voxel in MeV."""
+        L = lib()
+        assert L.ref_load(self.phys.ctypes.data, self.scene_ptr) == 0
+        nvox = self.sh.scene.nx * self.sh.scene.ny * self.sh.scene.nz
+        tally = np.zeros(nvox, np.float64)
+        over = L.ref_transport(h0, h1, seed, tally.ctypes.data, nvox)
+        if over != 0:
+            raise RuntimeError(f"reference transport: {over} stack overflows")
+        return tally
 
 
 def sort_by_stack(out, on):
