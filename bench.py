@@ -335,14 +335,80 @@ def make_job(args, histories):
     return W.config3(histories=histories, nphsp=args.nphsp)
 
 
+_REF_JOB = None
+_REF_SCENE = None
+_REF_PAIR = None
+
+
+def _ref_worker(rng):
+    """One process of the reference arm: histories [h0, h1) of the plan by the
+    reference's own kernels (forked from the parent, which holds the plan)."""
+    from oracle import refpin as R
+    global _REF_PAIR
+    h0, h1, seed = rng
+    if _REF_PAIR is None:                         # once per process: the reference's globals from the plan
+        _REF_PAIR = R.Pair(_REF_JOB.physics, _REF_SCENE)
+    pair = _REF_PAIR
+    t = time.perf_counter()
+    e = pair.transport(h0, h1, seed=seed)
+    return time.perf_counter() - t, float(e.sum())
+
+
+def run_reference_transport(args, job):
+    """The reference arm on the reference's own code: whole transports by its
+    ten stage kernels compiled as host code (oracle/_ref, ref_transport), one
+    process per host core, each on its own share of the step's histories.
+    Forked before anything touches CUDA. Returns the JSON line's fields."""
+    import multiprocessing as mp
+    global _REF_JOB, _REF_SCENE
+    _REF_JOB, _REF_SCENE = job, job.scene()
+    procs = os.cpu_count() or 1
+    ctx = mp.get_context("fork")
+    with ctx.Pool(procs) as pool:
+        # calibrate: a short run on every process, then size a step to about ref_seconds
+        per = 2000
+        dts = pool.map(_ref_worker, [(k * per, (k + 1) * per, 9000 + k) for k in range(procs)])
+        rate1 = per / max(np.median([d for d, _ in dts]), 1e-6)
+        per = max(2000, int(rate1 * args.ref_seconds))
+        step_hist = per * procs
+        per_step_ms = []
+        for s in range(args.warmup + args.steps):
+            base = (1 + s) * step_hist
+            t = time.perf_counter()
+            pool.map(_ref_worker, [(base + k * per, base + (k + 1) * per, 100 * s + k) for k in range(procs)])
+            if s >= args.warmup:
+                per_step_ms.append((time.perf_counter() - t) * 1e3)
+    value = step_hist * args.steps / (sum(per_step_ms) / 1e3)
+    return value, per_step_ms, step_hist, procs
+
+
 def run_reference(args):
-    """CPU restatement of the reference routines (the oracle) on all host cores."""
+    """The reference arm: the reference's own kernels on all host cores when its
+    sources compiled here (oracle/_ref), else the CPU restatement (the oracle)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import oracle as O
+    from oracle import refpin as R
     O.build()
+    R.build()
     job = make_job(args, 200_000_000)
+    if R.available():
+        value, per_step_ms, steps_hist, cores = run_reference_transport(args, job)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(per_step_ms)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "C3 synthetic CT head 256x256x120, 5 fields, jaws +-6 cm, 120-leaf MLC, 6 MV-like phsp",
+                       "hist_per_step": steps_hist, "parallelism": f"{cores} host processes"},
+            "cpu_baseline": {"value": value, "unit": "histories/s", "cores": cores, "kind": "reference",
+                             "sample": f"{steps_hist} C3 histories per step on {cores} processes: the reference's ten "
+                                       "stage kernels and geometry compiled from its sources as host code "
+                                       "(oracle/_ref, g++ -O2), draining their stacks, one process per core"},
+            "e2e": {"value": value, "unit": "histories/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
     rate, n, dt, cores = cpu_histories_per_s(job, seconds=args.ref_seconds)
     per_step_ms = []
     sh = job.scene()

@@ -57,6 +57,7 @@ def available() -> bool:
 
 
 _lib = None
+_loaded = None          # the Pair whose plan the harness's globals hold
 
 
 def lib():
@@ -147,12 +148,20 @@ class Pair(OraclePair):
 
     def __init__(self, physics, scene_holder):
         super().__init__(physics, scene_holder)
-        rc = lib().ref_load(self.phys.ctypes.data, self.scene_ptr)
-        if rc != 0:
-            raise RuntimeError("ref_load failed")
+        self._load()
+
+    def _load(self):
+        """Fill the harness's reference globals from this pair's plan (they are
+        per process, and the last pair made or used owns them)."""
+        global _loaded
+        if _loaded is not self:
+            if lib().ref_load(self.phys.ctypes.data, self.scene_ptr) != 0:
+                raise RuntimeError("ref_load failed")
+            _loaded = self
 
     def geom(self, parts, t_in):
         """howfar / hownear on both sides: {"ora": ..., "ref": ...}."""
+        self._load()
         parts = np.ascontiguousarray(parts, PARTICLE)
         t_in = np.ascontiguousarray(t_in, np.float32)
         n = len(parts)
@@ -166,6 +175,7 @@ class Pair(OraclePair):
     def stage(self, stage, parts, ucap=4096, ocap=64, dcap=4096):
         """One pass of `stage` per particle on both sides; the reference is fed
         the uniforms the oracle drew for each particle."""
+        self._load()
         parts = np.ascontiguousarray(parts, PARTICLE)
         n = len(parts)
         ora = super().stage(stage, parts, ucap, ocap, dcap)
@@ -183,6 +193,7 @@ class Pair(OraclePair):
 
     def uphi(self, which, a, b, part, cs=(0.0, 0.0)):
         """(oracle, reference) results of one rotation: particle and cos/sin pairs."""
+        self._load()
         po, co, u = super().uphi(which, a, b, part, cs)
         p = np.ascontiguousarray(np.array([part], PARTICLE))
         c = np.array([cs[0], cs[1], 0.0, 0.0], np.float32)
@@ -194,7 +205,7 @@ class Pair(OraclePair):
         CPU thread, a seeded generator for the random numbers): energy per
         voxel in MeV."""
         L = lib()
-        assert L.ref_load(self.phys.ctypes.data, self.scene_ptr) == 0
+        self._load()
         nvox = self.sh.scene.nx * self.sh.scene.ny * self.sh.scene.nz
         tally = np.zeros(nvox, np.float64)
         over = L.ref_transport(h0, h1, seed, tally.ctypes.data, nvox)
@@ -220,7 +231,9 @@ class Setup:
 
     def __init__(self, egsphant, mlc_egsinp, jaws_egsinp, mlcinfo, data_dir, sid, default_medium,
                  output_factor_file=None):
+        global _loaded
         L = lib()
+        _loaded = None                      # the set-up overwrites the reference's globals
         msg = C.create_string_buffer(512)
         d = str(data_dir).rstrip("/") + "/"          # the reference prepends it to each mlcinp name
         st = L.ref_setup_run(str(egsphant).encode(), str(mlc_egsinp).encode(), str(jaws_egsinp).encode(),
