@@ -298,3 +298,32 @@ def test_batch_uncertainty_splits_every_field_and_keeps_the_tally(tmp_path):
     name = F.write_uncertainty(str(tmp_path / "U"), sigma.astype(np.float32), 1, 2, 3)
     assert name.endswith("U_uncertianty_001x002x003.bin")
     np.testing.assert_array_equal(np.fromfile(name, np.float32), sigma.astype(np.float32))
+
+
+def test_reference_example_plans_parse():
+    """The reference's own example plans (Test*.ini beside its sources) read
+    with the package's INI rules: every section the reference reads is found,
+    numbers come out as the reference's sscanf("%f") gives them, and the
+    options this path refuses are recognised (CTcreate from DICOM)."""
+    from gegs_b200.plan import _floats, _get, _on
+    from oracle.refpin import REF_DIR
+    plans = sorted(REF_DIR.glob("Test*.ini")) if REF_DIR.is_dir() else []
+    if not plans:
+        pytest.skip("the reference's example plans are not present")
+    for path in plans:
+        ini = read_ini(path)
+        for sec in ("general", "data", "phase space", "secjaws", "mlc", "phantom"):
+            assert sec in ini, (path.name, sec)
+        h = _floats(_get(ini, "General", "histories", required=True), 1, "histories")[0]
+        assert h == float(np.float32(h)) and h >= 1
+        iso = _floats(_get(ini, "Phantom", "isocenter location", required=True), 3, "iso")
+        assert all(v == float(np.float32(v)) for v in iso)
+        sid = _floats(_get(ini, "Phantom", "source to isocenter", required=True), 1, "sid")[0]
+        assert sid > 0
+        z = _floats(_get(ini, "Phase space", "z position", required=True), 1, "z")[0]
+        assert z == float(np.float32(z))
+        assert "\\" in _get(ini, "Data", "data directory") or _get(ini, "Data", "data directory")
+        if _on(_get(ini, "Dose output", "relative dose")):
+            gl, gd = _floats(_get(ini, "Dose output", "gamma index (mm,%)", required=True), 2, "gamma")
+            assert gl > 0 and gd > 0
+        assert isinstance(_on(_get(ini, "CTcreate", "use ctcreate")), bool)
