@@ -620,9 +620,11 @@ def main():
         cpu = {"value": crate, "unit": "histories/s", "cores": cores, "kind": "port",
                "sample": f"{cn} C3 histories in {cdt:.1f} s on {cores} host threads (CPU oracle, same inputs)",
                "value_1_core": r1, "sample_1_core": f"{n1} C3 histories in {dt1:.1f} s on 1 thread"}
-    # per step: the first planner launch, then per wave the source, the stage kernels (the
-    # persistent form runs photon and electron transport as jaws + MLC + phantom kernels) and the planner
-    per_wave = 12 if args.mode == "plain" else 16
+    # per step: the first planner launch, then per wave the kernels of one wave and the planner.
+    # Plain form: source + 10 stage kernels + planner. Timed form: source, photon jaws / MLC /
+    # phantom, 4 photon interactions, electron jaws + near pass, MLC + near pass, phantom, 4
+    # electron interactions, planner. Persistent form: the same plus the long jaws-photon kernel.
+    per_wave = {"plain": 12, "timed": 18}.get(args.mode, 19)
     launches_per_step = [1 + per_wave * (st["waves"] - 1) for st in stats]
     line = {
         "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": world, "steps": args.steps,

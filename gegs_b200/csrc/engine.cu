@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -79,6 +80,7 @@ struct gegs_engine {
     DevCtx ctx{};
     bool have_physics = false, have_scene = false;
     unsigned long long ctx_gen = 1;
+    unsigned long long uid = 0;        // unique per engine of the process (group graph keys)
 
     // cached persistent graph
     // cached persistent graphs: slot 0 forward transport, slot 1 gradient replay
@@ -96,6 +98,7 @@ struct gegs_engine {
     gegs_run_stats last{};
     bool in_flight = false;            // gegs_launch queued a run that gegs_wait has not finished
     std::shared_ptr<struct GroupRun> group;   // the group graph this engine's launched run belongs to
+    std::shared_ptr<struct GroupRun> group_cache;   // the last group graph built with this engine
 
     // batch statistics (gegs_stat_*): per voxel the sum and sum of squares of
     // batch energies (MeV) and the tally at the last fold
@@ -172,6 +175,8 @@ gegs_status gegs_create(int device, gegs_engine **out)
     if (!out) return GEGS_ERR_ARG;
     *out = nullptr;
     gegs_engine *e = new gegs_engine();
+    static std::atomic<unsigned long long> next_uid{1};
+    e->uid = next_uid++;
     e->device = device;
     cudaError_t c = cudaSetDevice(device);
     if (c != cudaSuccess) { gegs_status s = cuda_fail(e, c, "cudaSetDevice"); *out = e; return s; }
@@ -576,8 +581,15 @@ static gegs_status build_graph(gegs_engine *e, int grid, int threads)
 
 // The executable graph of a group launch, shared by the group's engines and
 // destroyed when the last of them has waited for its run.
+struct GroupKey {
+    unsigned long long uid, gen;       // the engine (never reused) and its context generation
+    int grid, threads;
+    bool operator==(const GroupKey &o) const { return uid == o.uid && gen == o.gen && grid == o.grid && threads == o.threads; }
+};
+
 struct GroupRun {
     cudaGraphExec_t exec = nullptr;
+    std::vector<GroupKey> key;          // the engines, in order, with the state their branches were captured from
     ~GroupRun() { if (exec) cudaGraphExecDestroy(exec); }
 };
 
@@ -861,16 +873,26 @@ extern "C" gegs_status gegs_launch_group(gegs_engine *const *engines, int32_t n,
         if (st != GEGS_OK) return st;
     }
     gegs_engine *e = engines[0];          // errors are reported on the first engine
-    cudaGraph_t g;
-    CK(cudaGraphCreate(&g, 0), "graph create");
-    for (int i = 0; i < n; i++) {
-        gegs_status st = add_wave_loop(engines[i], g, R[i].grid, R[i].threads, true);
-        if (st != GEGS_OK) { cudaGraphDestroy(g); if (engines[i] != e) e->err = engines[i]->err; return st; }
+    // the same engines in the same state as the last group launch reuse its graph
+    std::vector<GroupKey> key(n);
+    for (int i = 0; i < n; i++) key[i] = GroupKey{engines[i]->uid, engines[i]->ctx_gen, R[i].grid, R[i].threads};
+    std::shared_ptr<GroupRun> grp = e->group_cache;
+    bool reuse = grp && grp->key == key;
+    for (int i = 1; reuse && i < n; i++) reuse = engines[i]->group_cache == grp;
+    if (!reuse) {
+        cudaGraph_t g;
+        CK(cudaGraphCreate(&g, 0), "graph create");
+        for (int i = 0; i < n; i++) {
+            gegs_status st = add_wave_loop(engines[i], g, R[i].grid, R[i].threads, true);
+            if (st != GEGS_OK) { cudaGraphDestroy(g); if (engines[i] != e) e->err = engines[i]->err; return st; }
+        }
+        grp = std::make_shared<GroupRun>();
+        cudaError_t ce = cudaGraphInstantiate(&grp->exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) { e->err = std::string("group graph instantiate: ") + cudaGetErrorString(ce); return GEGS_ERR_CUDA; }
+        grp->key = key;
+        for (int i = 0; i < n; i++) engines[i]->group_cache = grp;
     }
-    auto grp = std::make_shared<GroupRun>();
-    cudaError_t ce = cudaGraphInstantiate(&grp->exec, g, 0);
-    cudaGraphDestroy(g);
-    if (ce != cudaSuccess) { e->err = std::string("group graph instantiate: ") + cudaGetErrorString(ce); return GEGS_ERR_CUDA; }
     // the group runs on the first engine's stream once every engine's set-up is done
     cudaStream_t s = e->stream;
     for (int i = 1; i < n; i++) {

@@ -139,6 +139,8 @@ gegs_status gegs_wait(gegs_engine *e);
  * may be NULL) as one CUDA graph, one branch per engine -- its planner, then
  * its wave loop -- launched once on the first engine's stream. Each engine is
  * then finished with gegs_wait; its device_ms is the time of the whole group.
+ * The graph is kept and launched again when the same engines, in the same
+ * order and state, are grouped next.
  * The reference runs plans and fields one after another (CUDA_EGS.cu:1715-1742). */
 gegs_status gegs_launch_group(gegs_engine *const *engines, int32_t n, const uint64_t *hist_begin,
                               const uint64_t *hist_end, const gegs_run_opts *opts);

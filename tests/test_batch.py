@@ -52,8 +52,12 @@ def test_one_launch_equals_launches_per_plan_and_the_oracle(oracle):
     pb = PlanBatch(jobs, memory_budget_gb=4.0)
     st = pb.run(one_launch=True)
     one = pb.tallies()
+    pb.run(one_launch=True)                                          # the cached group graph again
+    again = pb.tallies()
     pb.run(one_launch=False)
     per = pb.tallies()
+    for a, b in zip(one, again):
+        np.testing.assert_array_equal(a, b)
     for a, b, s in zip(one, per, st):
         np.testing.assert_array_equal(a, b)
         assert s["error_bits"] == 0 and a.sum() > 0 and s["waves"] > 0
