@@ -540,14 +540,17 @@ def main():
         pinned = np.empty(rec_per_step * 28, np.uint8)
     from gegs_b200.scene import PHSP_DTYPE
     chunk = pinned.view(PHSP_DTYPE)
-    host_tally = np.empty(eng.nvox, np.int64)
+    try:
+        host_tally = torch.empty((eng.nvox,), dtype=torch.int64).pin_memory().numpy()
+    except Exception:
+        host_tally = np.empty(eng.nvox, np.int64)
     for s in range(args.steps):
         j0 = (s * rec_per_step) % max(1, len(job.phsp) - rec_per_step)
         chunk[:] = job.phsp[j0:j0 + rec_per_step]
         t = time.perf_counter()
         eng.set_phsp(chunk)
         eng.run(*hist_range(args.warmup + s), **ropt)
-        host_tally[:] = eng.tally()
+        eng.tally(out=host_tally)
         e2e_ms.append((time.perf_counter() - t) * 1e3)
     e2e = H * args.steps * world / (sum(e2e_ms) / 1e3)
     if dist is not None:

@@ -220,8 +220,13 @@ class Engine:
     def reset_tally(self):
         self._check(self.L.gegs_reset_tally(self.h))
 
-    def tally(self) -> np.ndarray:
-        out = np.zeros(self.nvox, np.int64)
+    def tally(self, out=None) -> np.ndarray:
+        """The int64 tally (MeV * 2^30 per voxel); into `out` when given (a
+        pinned host buffer makes the copy a direct DMA)."""
+        if out is None:
+            out = np.empty(self.nvox, np.int64)
+        elif out.dtype != np.int64 or out.size != self.nvox or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous int64 array of nvox values")
         self._check(self.L.gegs_get_tally(self.h, out.ctypes.data, self.nvox))
         return out
 
