@@ -42,7 +42,8 @@ static_assert(GX_NQ == GEGS_NQUEUES, "gegs_run_stats reports every queue");
 struct gegs_engine {
     int device = 0;
     int nsm = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;     // the stream all of the engine's work goes on
+    cudaStream_t own_stream = nullptr; // the engine's own (stream, unless gegs_set_stream named another)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // side streams and events that fork the independent kernels of a wave into
     // parallel branches of the persistent graph
@@ -181,7 +182,8 @@ gegs_status gegs_create(int device, gegs_engine **out)
     cudaError_t c = cudaSetDevice(device);
     if (c != cudaSuccess) { gegs_status s = cuda_fail(e, c, "cudaSetDevice"); *out = e; return s; }
     cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, device);
-    CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "stream");
+    CK(cudaStreamCreateWithFlags(&e->own_stream, cudaStreamNonBlocking), "stream");
+    e->stream = e->own_stream;
     CK(cudaEventCreate(&e->ev0), "event");
     CK(cudaEventCreate(&e->ev1), "event");
     for (int k = 0; k < 3; k++) {
@@ -220,7 +222,7 @@ void gegs_destroy(gegs_engine *e)
         if (e->ev_join[k]) cudaEventDestroy(e->ev_join[k]);
     }
     if (e->ev_fork) cudaEventDestroy(e->ev_fork);
-    if (e->stream) cudaStreamDestroy(e->stream);
+    if (e->own_stream) cudaStreamDestroy(e->own_stream);
     delete e;
 }
 
@@ -849,6 +851,16 @@ extern "C" gegs_status gegs_wait(gegs_engine *e)
     if (!e->in_flight) { e->err = "gegs_wait: no launched run"; return GEGS_ERR_ARG; }
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     return run_finish(e);
+}
+
+extern "C" gegs_status gegs_set_stream(gegs_engine *e, void *cuda_stream)
+{
+    if (!e) return GEGS_ERR_ARG;
+    if (e->in_flight) { e->err = "a launched run has not been waited for (gegs_wait)"; return GEGS_ERR_ARG; }
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(e->stream), "stream sync");      // work queued on the previous stream first
+    e->stream = cuda_stream ? (cudaStream_t)cuda_stream : e->own_stream;
+    return GEGS_OK;
 }
 
 extern "C" gegs_status gegs_launch_group(gegs_engine *const *engines, int32_t n, const uint64_t *hist_begin,

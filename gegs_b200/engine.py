@@ -20,7 +20,7 @@ MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 
 EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_set_timeline", "gegs_get_timeline", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
            "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_set_tally", "gegs_get_dose", "gegs_get_stats",
-           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_launch_group", "gegs_probe_geometry", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version",
+           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_launch_group", "gegs_probe_geometry", "gegs_set_stream", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version",
            "gegs_check_physics", "gegs_stat_begin", "gegs_stat_fold", "gegs_stat_get"]
 
 
@@ -81,6 +81,7 @@ def load_library(path=None):
     L.gegs_wait.argtypes = [vp]
     L.gegs_launch_group.argtypes = [vp, C.c_int32, vp, vp, vp]
     L.gegs_probe_geometry.argtypes = [vp, C.c_uint32, vp, vp, vp, vp, vp, vp]
+    L.gegs_set_stream.argtypes = [vp, vp]
     L.gegs_set_beamlet_weights.argtypes = [vp, vp, C.c_uint32]
     L.gegs_backward.argtypes = [vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint32, C.POINTER(RunOpts)]
     L.gegs_reset_tally.argtypes = [vp]
@@ -194,6 +195,12 @@ class Engine:
     def wait(self):
         self._check(self.L.gegs_wait(self.h))
         return self.stats()
+
+    def set_stream(self, stream=None):
+        """Issue the engine's work on a caller's CUDA stream (a torch.cuda.Stream
+        or a raw cudaStream_t handle); None returns to the engine's own."""
+        handle = getattr(stream, "cuda_stream", stream)
+        self._check(self.L.gegs_set_stream(self.h, handle))
 
     def probe_geometry(self, states, t_in):
         """howfar (step t_in) and hownear of each state on the device

@@ -134,6 +134,13 @@ gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, con
 gegs_status gegs_launch(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts);
 gegs_status gegs_wait(gegs_engine *e);
 
+/* The CUDA stream (a cudaStream_t of the engine's device, passed as a pointer)
+ * on which the engine issues all of its work from now on, so that a caller can
+ * order it with its own work; NULL returns to the engine's own stream. The
+ * caller keeps the stream alive while the engine uses it. (The reference has
+ * no streams: runSimulation synchronises after every kernel, CUDA_EGS.cu:226-365.) */
+gegs_status gegs_set_stream(gegs_engine *e, void *cuda_stream);
+
 /* Several plans in one launch: the persistent-form runs of n engines on one
  * device (engine i transports [hist_begin[i], hist_end[i]) with opts[i]; opts
  * may be NULL) as one CUDA graph, one branch per engine -- its planner, then

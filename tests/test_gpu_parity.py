@@ -165,3 +165,25 @@ def test_tables_staged_in_shared_memory_bit_exact(engine, oracle):
     engine.reset_tally()
     engine.run(0, job.histories, mode=2, stage_tables=True)          # the timed form launches them by name
     _assert_same(engine.tally(), ref)
+
+
+@pytest.mark.gpu
+def test_run_on_a_callers_stream(engine, oracle):
+    """gegs_set_stream: the engine's work goes on the caller's stream; the
+    tally is the same, and the engine returns to its own stream after."""
+    import torch
+    job = W.config1(histories=3000, n=16, voxel=2.0)
+    sh = job.scene()
+    engine.set_physics(job.physics)
+    engine.set_scene(sh)
+    s = torch.cuda.Stream(device=0)
+    engine.set_stream(s)
+    engine.reset_tally()
+    engine.run(0, job.histories)
+    got = engine.tally()
+    engine.set_stream(None)
+    ref, _ = oracle.run(job.physics, sh, 0, job.histories)
+    np.testing.assert_array_equal(got, ref)
+    engine.reset_tally()
+    engine.run(0, job.histories)
+    np.testing.assert_array_equal(engine.tally(), ref)
