@@ -82,6 +82,8 @@ struct gegs_engine {
     bool have_physics = false, have_scene = false;
     unsigned long long ctx_gen = 1;
     unsigned long long uid = 0;        // unique per engine of the process (group graph keys)
+    std::vector<gegs_field> host_fields;   // the scene's fields as last set (gegs_set_field)
+    int nfields = 0;
 
     // cached persistent graph
     // cached persistent graphs: slot 0 forward transport, slot 1 gradient replay
@@ -333,6 +335,8 @@ gegs_status gegs_set_scene(gegs_engine *e, const gegs_scene *S)
     CK(cudaMemcpy(e->d_xb, S->x_bounds, ((size_t)S->nx + 1) * 4, cudaMemcpyHostToDevice), "bounds H2D");
     CK(cudaMemcpy(e->d_yb, S->y_bounds, ((size_t)S->ny + 1) * 4, cudaMemcpyHostToDevice), "bounds H2D");
     CK(cudaMemcpy(e->d_zb, S->z_bounds, ((size_t)S->nz + 1) * 4, cudaMemcpyHostToDevice), "bounds H2D");
+    e->host_fields.assign(S->fields, S->fields + S->nfields);
+    e->nfields = S->nfields;
     CK(realloc_dev(&e->d_fields, (size_t)S->nfields), "fields");
     CK(cudaMemcpy(e->d_fields, S->fields, sizeof(gegs_field) * S->nfields, cudaMemcpyHostToDevice), "fields H2D");
     {
@@ -851,6 +855,25 @@ extern "C" gegs_status gegs_wait(gegs_engine *e)
     if (!e->in_flight) { e->err = "gegs_wait: no launched run"; return GEGS_ERR_ARG; }
     CK(cudaSetDevice(e->device), "cudaSetDevice");
     return run_finish(e);
+}
+
+extern "C" gegs_status gegs_set_field(gegs_engine *e, int32_t index, const gegs_field *F)
+{
+    if (!e || !F || !e->have_scene || index < 0 || index >= e->nfields) return GEGS_ERR_ARG;
+    if (e->in_flight) { e->err = "a launched run has not been waited for (gegs_wait)"; return GEGS_ERR_ARG; }
+    if (F->nrepeat < 0 || F->nrepeat > 255 || F->hist_end < F->hist_begin) {
+        e->err = "gegs_set_field: bad history range or recycling count";
+        return GEGS_ERR_ARG;
+    }
+    CK(cudaSetDevice(e->device), "cudaSetDevice");
+    e->host_fields[(size_t)index] = *F;
+    std::vector<float4> lines = jaw_edge_lines(e->host_fields.data(), e->nfields);
+    // the device arrays keep their addresses: graphs built before stay valid
+    CK(cudaMemcpyAsync(e->d_fields + index, F, sizeof(gegs_field), cudaMemcpyHostToDevice, e->stream), "field H2D");
+    CK(cudaMemcpyAsync(e->d_jaw_lines, lines.data(), lines.size() * sizeof(float4), cudaMemcpyHostToDevice, e->stream),
+       "jaw lines H2D");
+    CK(cudaStreamSynchronize(e->stream), "field sync");
+    return GEGS_OK;
 }
 
 extern "C" gegs_status gegs_set_stream(gegs_engine *e, void *cuda_stream)

@@ -20,7 +20,7 @@ MODE_PERSISTENT, MODE_PLAIN, MODE_TIMED = 0, 1, 2
 
 EXPORTS = ["gegs_set_trace", "gegs_get_trace", "gegs_set_timeline", "gegs_get_timeline", "gegs_create", "gegs_destroy", "gegs_last_error", "gegs_set_physics", "gegs_set_scene", "gegs_set_phsp",
            "gegs_run", "gegs_reset_tally", "gegs_get_tally", "gegs_set_tally", "gegs_get_dose", "gegs_get_stats",
-           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_launch_group", "gegs_probe_geometry", "gegs_set_stream", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version",
+           "gegs_tally_device_ptr", "gegs_run_noalloc", "gegs_launch", "gegs_wait", "gegs_launch_group", "gegs_probe_geometry", "gegs_set_stream", "gegs_set_field", "gegs_set_beamlet_weights", "gegs_backward", "gegs_sizeof_physics", "gegs_sizeof_scene", "gegs_sizeof_field", "gegs_version",
            "gegs_check_physics", "gegs_stat_begin", "gegs_stat_fold", "gegs_stat_get"]
 
 
@@ -82,6 +82,7 @@ def load_library(path=None):
     L.gegs_launch_group.argtypes = [vp, C.c_int32, vp, vp, vp]
     L.gegs_probe_geometry.argtypes = [vp, C.c_uint32, vp, vp, vp, vp, vp, vp]
     L.gegs_set_stream.argtypes = [vp, vp]
+    L.gegs_set_field.argtypes = [vp, C.c_int32, vp]
     L.gegs_set_beamlet_weights.argtypes = [vp, vp, C.c_uint32]
     L.gegs_backward.argtypes = [vp, C.c_uint64, C.c_uint64, vp, vp, C.c_uint32, C.POINTER(RunOpts)]
     L.gegs_reset_tally.argtypes = [vp]
@@ -195,6 +196,13 @@ class Engine:
     def wait(self):
         self._check(self.L.gegs_wait(self.h))
         return self.stats()
+
+    def set_field(self, index: int, field: dict):
+        """Replace one field of the scene (gegs_set_field): angle, history range,
+        jaw and leaf-end polygons, as a field dict of a job."""
+        from .scene import Field, fill_field
+        F = fill_field(Field(), field)
+        self._check(self.L.gegs_set_field(self.h, index, C.byref(F)))
 
     def set_stream(self, stream=None):
         """Issue the engine's work on a caller's CUDA stream (a torch.cuda.Stream

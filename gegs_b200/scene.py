@@ -64,6 +64,19 @@ def _ptr(a, ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
 
+def fill_field(F, f):
+    """A gegs_field from a field dict (cos_angle, sin_angle, hist_begin,
+    hist_end, nrepeat and the polygons the field has)."""
+    F.cos_angle, F.sin_angle = f["cos_angle"], f["sin_angle"]
+    F.hist_begin, F.hist_end = int(f["hist_begin"]), int(f["hist_end"])
+    F.nrepeat = int(f["nrepeat"])
+    for k in ("boundMinY", "boundMinX", "boundMaxY", "boundMaxX", "jawsGeomY", "jawsGeomX", "endnode"):
+        if k in f:
+            a = np.ascontiguousarray(f[k], np.float32)
+            C.memmove(C.addressof(getattr(F, k)), a.ctypes.data, a.nbytes)
+    return F
+
+
 class SceneHolder:
     """A filled :class:`Scene` plus the numpy arrays its pointers refer to."""
 
@@ -105,14 +118,7 @@ class SceneHolder:
             raise ValueError(f"1..{MAX_FIELDS} fields, got {nf}")
         farr = (Field * nf)()
         for i, f in enumerate(fields):
-            F = farr[i]
-            F.cos_angle, F.sin_angle = f["cos_angle"], f["sin_angle"]
-            F.hist_begin, F.hist_end = int(f["hist_begin"]), int(f["hist_end"])
-            F.nrepeat = int(f["nrepeat"])
-            for k in ("boundMinY", "boundMinX", "boundMaxY", "boundMaxX", "jawsGeomY", "jawsGeomX", "endnode"):
-                if k in f:
-                    a = np.ascontiguousarray(f[k], np.float32)
-                    C.memmove(C.addressof(getattr(F, k)), a.ctypes.data, a.nbytes)
+            fill_field(farr[i], f)
         self.fields_arr = farr
         s.nfields = nf
         s.fields = C.cast(farr, C.POINTER(Field))

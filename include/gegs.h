@@ -134,6 +134,12 @@ gegs_status gegs_run(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, con
 gegs_status gegs_launch(gegs_engine *e, uint64_t hist_begin, uint64_t hist_end, const gegs_run_opts *opts);
 gegs_status gegs_wait(gegs_engine *e);
 
+/* Replace field `index` of the scene (its gantry cosine and sine, history range,
+ * recycling count, jaw and leaf-end polygons) without uploading the phantom
+ * again; the tally is kept. The reference sets a field up before each field's
+ * run (setup_secjaws, init_leaf_pos, CUDA_EGS.cu:416-432). */
+gegs_status gegs_set_field(gegs_engine *e, int32_t index, const gegs_field *F);
+
 /* The CUDA stream (a cudaStream_t of the engine's device, passed as a pointer)
  * on which the engine issues all of its work from now on, so that a caller can
  * order it with its own work; NULL returns to the engine's own stream. The

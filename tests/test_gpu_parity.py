@@ -187,3 +187,25 @@ def test_run_on_a_callers_stream(engine, oracle):
     engine.reset_tally()
     engine.run(0, job.histories)
     np.testing.assert_array_equal(engine.tally(), ref)
+
+
+@pytest.mark.gpu
+def test_set_field_equals_a_new_scene(engine, oracle):
+    """gegs_set_field: new leaf positions and jaws for one field, set without
+    uploading the phantom again, give the tally of a scene built with them."""
+    from gegs_b200 import geometry as G
+    job = W.config3(histories=3000, nphsp=3000, dims=(32, 32, 16))
+    engine.set_physics(job.physics)
+    engine.set_scene(job.scene())
+    f = dict(job.fields[2])
+    pos = np.asarray(f["leaf_pos"], np.float32) + np.float32(0.7)          # every leaf pair opened by 1.4 cm
+    f["leaf_pos"] = pos
+    f["endnode"] = G.leaf_endnodes(job.beam["mlc"]["crossYZ"], pos, job.beam["mlc"]["zmin"],
+                                   job.beam["mlc"]["zthick"], job.beam["source_to_isocenter"])
+    f.update(G.secjaws_polygons(job.meta["jaws"], -4.0, 5.0, -3.0, 4.0, job.beam["source_to_isocenter"]))
+    engine.set_field(2, f)
+    engine.reset_tally()
+    engine.run(0, job.histories)
+    job.fields[2] = f
+    ref, _ = oracle.run(job.physics, job.scene(), 0, job.histories)
+    np.testing.assert_array_equal(engine.tally(), ref)
