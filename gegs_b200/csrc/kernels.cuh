@@ -238,6 +238,10 @@ __device__ __forceinline__ bool refill(const DevCtx &C, int hq, uint32_t n_cont,
 #ifndef GX_EPHANTOM_MIN_BLOCKS
 #define GX_EPHANTOM_MIN_BLOCKS 4
 #endif
+// the jaws photons (and their long tracks): 48 registers, 0.3 % faster than 64
+#ifndef GX_PJAWS_MIN_BLOCKS
+#define GX_PJAWS_MIN_BLOCKS 5
+#endif
 // the MLC photon kernel, the most divergent, runs best with 80 registers (fewer spills)
 #ifndef GX_PMLC_MIN_BLOCKS
 #define GX_PMLC_MIN_BLOCKS 3
@@ -362,12 +366,12 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     timeline_mark(C, tl, true);
 }
 
-__global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_jaws(const __grid_constant__ DevCtx C)
+__global__ void __launch_bounds__(256, GX_PJAWS_MIN_BLOCKS) k_photon_jaws(const __grid_constant__ DevCtx C)
 {
     transport_consumer<false, GX_GEOM_JAWS>(C);
 }
 
-__global__ void __launch_bounds__(256, GX_PHOTON_MIN_BLOCKS) k_photon_jaws_long(const __grid_constant__ DevCtx C)
+__global__ void __launch_bounds__(256, GX_PJAWS_MIN_BLOCKS) k_photon_jaws_long(const __grid_constant__ DevCtx C)
 {
     transport_consumer<false, GX_GEOM_JAWS, true>(C);
 }
