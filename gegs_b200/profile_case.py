@@ -89,6 +89,17 @@ def timeline_summary(eng, args, dims):
     pj = dur[:, 1]
     others = np.max(np.delete(dur, [1], axis=1), axis=1)
     lone = (pj > 0.5) & (pj > 2 * others)
+    # per wave: span from its first kernel start to its last kernel end, the
+    # phases' spans inside it, and the gap to the next wave (the planner node
+    # and the graph's conditional hand-over)
+    live = ran.any(axis=1)
+    ws, we = np.nanmin(s[live], axis=1), np.nanmax(e[live], axis=1)
+    wave_ms = we - ws
+    gap_ms = np.maximum(ws[1:] - we[:-1], 0.0)
+    with np.errstate(all="ignore"), warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        per_phase = {k: np.round(span(g)[live], 3).tolist() for k, g in groups.items()}
+    small = wave_ms < 1.0
     return {"workload": f"C3 CT head {dims[0]}x{dims[1]}x{dims[2]}, 5 fields, persistent form",
             "histories": args.histories, "first": args.first, "batch": args.batch or "auto",
             "device_ms": st["device_ms"], "waves": st["waves"],
@@ -97,7 +108,10 @@ def timeline_summary(eng, args, dims):
             "serial_overlap": "kernel sums exceed phase spans where kernels of a phase overlap",
             "lone_photon_jaws_waves": int(lone.sum()),
             "lone_photon_jaws_ms": round(float(pj[lone].sum()), 1),
-            "longest_photon_jaws_ms": [round(float(x), 2) for x in np.sort(pj)[::-1][:5]]}
+            "longest_photon_jaws_ms": [round(float(x), 2) for x in np.sort(pj)[::-1][:5]],
+            "waves_under_1ms": int(small.sum()), "waves_under_1ms_ms": round(float(wave_ms[small].sum()), 1),
+            "gaps_between_waves_ms": round(float(gap_ms.sum()), 1),
+            "wave_ms": np.round(wave_ms, 3).tolist(), "wave_phase_ms": per_phase}
 
 
 if __name__ == "__main__":

@@ -70,3 +70,5 @@ def test_timeline_summary_sums_phases_and_kernels():
     assert d["phase_ms"]["electron transport"] == 2.0
     assert d["kernel_ms"]["photon_jaws"] == 4.0 and d["kernel_ms"]["photon"] == 3.0
     assert d["lone_photon_jaws_waves"] == 1 and d["lone_photon_jaws_ms"] == 2.0
+    assert d["wave_ms"] == [7.0, 2.0] and d["gaps_between_waves_ms"] == 1.0
+    assert d["waves_under_1ms"] == 0 and d["wave_phase_ms"]["photon transport"] == [3.0, 2.0]
