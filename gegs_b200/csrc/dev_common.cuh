@@ -183,6 +183,9 @@ struct DevCtx {
     uint32_t *photon_done;          // photon MLC and phantom consumers finished in this wave
     uint32_t *electron_done;        // electron branches (jaws, MLC, phantom) finished in this wave
     uint32_t overlap;               // 1: a phase's class consumers run as concurrent graph branches
+    uint32_t pipelined;             // 1: a wave runs both transport phases at once, then both interaction
+                                    // phases (persistent form); a positron that stops in the electron
+                                    // transport annihilates at rest in the annihilation kernel
     uint32_t photon_budget, electron_budget;   // steps per particle per launch before continuation
     unsigned long long *timeline;   // [timeline_waves][16][2] first start / last end (ns) per kernel; null: off
     uint32_t timeline_waves;

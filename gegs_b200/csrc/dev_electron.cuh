@@ -239,10 +239,22 @@ __device__ __forceinline__ void estate_init(EState &s)
     s.lelke = 0; s.compute_tstep = true; s.is_tstep = true;
 }
 
+// A positron at rest handed to the annihilation kernel carries energy 0 (one
+// annihilating in flight carries its total energy, above the rest mass).
+__device__ __forceinline__ bool at_rest_mark(const Part &p) { return p.e == 0.0f; }
+
 __device__ __forceinline__ void e_discard_below_cut(const DevCtx &C, Part &p, const RegInfo &rd, Rng &r)
 {
     escore(C, p, p.region, (p.e - C.P->prm) * p.wt);
-    if (p.charge > 0) annih_at_rest(C, p, rd, r);
+    if (p.charge > 0) {
+        if (C.pipelined) {
+            // the photon transport of this wave runs beside this kernel and takes
+            // no new photons: the annihilation kernel, after both transports,
+            // makes them from the same random stream (region_info(p.region) is rd)
+            p.e = 0.0f;
+            push_move(C, ST_ANNIH, p, r);
+        } else annih_at_rest(C, p, rd, r);
+    }
 }
 
 // One iteration of the ELECTR loop.  Returns true when the particle has left

@@ -39,6 +39,10 @@ constexpr unsigned long long estate_factor_sum()
 
 static_assert(GX_NQ == GEGS_NQUEUES, "gegs_run_stats reports every queue");
 
+// side streams of the graph's parallel branches (the pipelined wave forks
+// eight interaction kernels: the engine's stream and seven more)
+static constexpr int kAux = 7;
+
 struct gegs_engine {
     int device = 0;
     int nsm = 0;
@@ -47,8 +51,8 @@ struct gegs_engine {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // side streams and events that fork the independent kernels of a wave into
     // parallel branches of the persistent graph
-    cudaStream_t aux[3] = {};
-    cudaEvent_t ev_fork = nullptr, ev_join[3] = {};
+    cudaStream_t aux[kAux] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kAux] = {};
     std::string err;
 
     gegs_physics *d_P = nullptr;
@@ -188,7 +192,7 @@ gegs_status gegs_create(int device, gegs_engine **out)
     e->stream = e->own_stream;
     CK(cudaEventCreate(&e->ev0), "event");
     CK(cudaEventCreate(&e->ev1), "event");
-    for (int k = 0; k < 3; k++) {
+    for (int k = 0; k < kAux; k++) {
         CK(cudaStreamCreateWithFlags(&e->aux[k], cudaStreamNonBlocking), "stream");
         CK(cudaEventCreateWithFlags(&e->ev_join[k], cudaEventDisableTiming), "event");
     }
@@ -219,7 +223,7 @@ void gegs_destroy(gegs_engine *e)
     for (int k = 0; k < GX_NESTATE; k++) cudaFree(e->d_estate[k]);
     if (e->ev0) cudaEventDestroy(e->ev0);
     if (e->ev1) cudaEventDestroy(e->ev1);
-    for (int k = 0; k < 3; k++) {
+    for (int k = 0; k < kAux; k++) {
         if (e->aux[k]) cudaStreamDestroy(e->aux[k]);
         if (e->ev_join[k]) cudaEventDestroy(e->ev_join[k]);
     }
@@ -505,8 +509,36 @@ static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
         }
     };
     k_source<<<grid, threads, 0, s>>>(C, e->d_sched);
-    fork(2);
     const size_t ps = C.stage_tables ? photon_smem_bytes(C.nmed) : 0;   // the staged {gmfp, cohe} table
+    if (C.pipelined) {
+        // Both transport phases at once: the photon consumers read the photon
+        // queues, the electron consumers the electron queues, and neither
+        // pushes to a queue the other reads (a positron stopping in the
+        // electron transport goes to the annihilation queue). Then all eight
+        // interaction kernels, whose new particles the next wave transports.
+        fork(5);
+        k_photon_jaws<<<grid, threads, ps, a[0]>>>(C);
+        k_photon_mlc<<<grid, threads, ps, a[1]>>>(C);
+        k_electron_jaws<<<grid, threads, 0, a[2]>>>(C);
+        k_electron_jaws_near<<<grid, threads, 0, a[2]>>>(C);
+        k_electron_mlc<<<grid, threads, 0, a[3]>>>(C);
+        k_electron_mlc_near<<<grid, threads, 0, a[3]>>>(C);
+        k_electron<<<grid, threads, 0, a[4]>>>(C);
+        k_photon<<<grid, threads, ps, s>>>(C);
+        join(5);
+        fork(7);
+        k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(C);
+        k_interact<ST_PHOTO><<<grid, threads, 0, a[0]>>>(C);
+        k_interact<ST_RAYLEIGH><<<grid, threads, 0, a[1]>>>(C);
+        k_interact<ST_PAIR><<<grid, threads, 0, a[2]>>>(C);
+        k_interact<ST_MOLLER><<<grid, threads, 0, a[3]>>>(C);
+        k_interact<ST_BREMS><<<grid, threads, 0, a[4]>>>(C);
+        k_interact<ST_BHABHA><<<grid, threads, 0, a[5]>>>(C);
+        k_interact<ST_ANNIH><<<grid, threads, 0, a[6]>>>(C);
+        join(7);
+        return;
+    }
+    fork(2);
     k_photon_jaws<<<grid, threads, ps, a[0]>>>(C);
     k_photon_mlc<<<grid, threads, ps, a[1]>>>(C);
     k_photon<<<grid, threads, ps, s>>>(C);
@@ -628,6 +660,8 @@ static gegs_status prepare_run(gegs_engine *e, uint64_t hist_begin, uint64_t his
     uint32_t max_waves = o.max_waves ? o.max_waves : 200000u;
     const uint32_t stage = (o.flags & GEGS_RUN_STAGE_TABLES) ? 1u : 0u;
     if (stage != e->ctx.stage_tables) { e->ctx.stage_tables = stage; e->ctx_gen++; }
+    const uint32_t pipe = (o.mode == GEGS_MODE_PERSISTENT && (o.flags & GEGS_RUN_PIPELINED)) ? 1u : 0u;
+    if (pipe != e->ctx.pipelined) { e->ctx.pipelined = pipe; e->ctx_gen++; }
     uint32_t pb = (o.step_budget & 0xFFFFu) ? (o.step_budget & 0xFFFFu) : 32u;
     uint32_t eb = (o.step_budget >> 16) ? (o.step_budget >> 16) : 4u;
     if (pb != e->ctx.photon_budget || eb != e->ctx.electron_budget) {
@@ -1219,6 +1253,7 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
     c.photon_done = &sched->photon_done;
     c.electron_done = &sched->electron_done;
     c.overlap = 0u;                 // one kernel at a time
+    c.pipelined = 0u;
     c.timeline = nullptr;
     c.timeline_waves = 0;
     c.trace = nullptr;

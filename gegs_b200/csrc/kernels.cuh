@@ -300,12 +300,15 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
     // advances with the bulk of the work instead of one budget per wave in the
     // run's tail. Only when the phase's kernels run concurrently (C.overlap).
     constexpr bool JAWS_PHOTON = !ELEC && G == GX_GEOM_JAWS;
+    // In the pipelined form the jaws photons step on while any of the five
+    // other transport branches of the wave (both particle types) still runs.
     const volatile uint32_t *others_done = LONG ? C.electron_done : C.photon_done;
-    constexpr uint32_t others = LONG ? 3u : 2u;
-    // in the persistent form, a jaws photon still going when the photon phase
-    // ends moves on to the long-track kernel, which runs beside the electron
-    // phase the same way
-    const int q_limit = (JAWS_PHOTON && !LONG && C.overlap) ? GX_Q_PLONG : qc_out;
+    const volatile uint32_t *others_done2 = C.electron_done;
+    const uint32_t others = LONG ? 3u : C.pipelined ? 5u : 2u;
+    // in the serial persistent form, a jaws photon still going when the photon
+    // phase ends moves on to the long-track kernel, which runs beside the
+    // electron phase the same way
+    const int q_limit = (JAWS_PHOTON && !LONG && C.overlap && !C.pipelined) ? GX_Q_PLONG : qc_out;
     Part p;
     Rng r;
     EState s;
@@ -345,7 +348,8 @@ __device__ __forceinline__ void transport_consumer(const DevCtx &C)
                 if (done) active = false;
                 else if (++nst >= budget &&
                          (!JAWS_PHOTON || !C.overlap || nst >= 64u * budget ||
-                          (((nst - budget) & 15u) == 0u && *others_done >= others))) {
+                          (((nst - budget) & 15u) == 0u &&
+                           *others_done + (C.pipelined && !LONG ? *others_done2 : 0u) >= others))) {
                     if (ELEC) { EStatePk k = pack_estate(s); push_cont(C, qc_out, p, r, &k); }
                     else push_cont(C, q_limit, p, r, nullptr);
                     active = false;
@@ -421,7 +425,20 @@ __device__ __forceinline__ void run_interaction(const DevCtx &C, const Part &p, 
     else if (Q == ST_MOLLER) moller(C, p, r);
     else if (Q == ST_BREMS) brems(C, p, r);
     else if (Q == ST_BHABHA) bhabha(C, p, r);
-    else if (Q == ST_ANNIH) annih(C, p, r);
+    else if (Q == ST_ANNIH) {
+        if (at_rest_mark(p)) {
+            Part q = p;
+            annih_at_rest(C, q, region_info(C, q.region), r);
+        } else annih(C, p, r);
+    }
+}
+
+// Entries an interaction kernel counts as processed: all but the positrons
+// handed over at rest (counted nowhere in the serial form either).
+template <int Q>
+__device__ __forceinline__ unsigned counted(const Part &p)
+{
+    return (Q == ST_ANNIH && at_rest_mark(p)) ? 0u : 1u;
 }
 
 template <int Q>
@@ -438,7 +455,7 @@ __global__ void __launch_bounds__(256) k_interact(const __grid_constant__ DevCtx
         rng_window(C, r);
         trace_event(C, 1u, Q, p);
         run_interaction<Q>(C, p, r);
-        taken++;
+        taken += counted<Q>(p);
     }
     block_stat_add(C, Q, taken);
     consumer_done(C, Q);
@@ -458,7 +475,7 @@ __global__ void __launch_bounds__(256) k_plain(const __grid_constant__ DevCtx C)
         Rng r;
         rng_load(r, p);
         trace_event(C, 1u, Q, p);
-        taken++;
+        taken += counted<Q>(p);
         if (Q == ST_PHOTON) {
             uint32_t nst = 0;
             while (!photon_step(C, p, r)) {

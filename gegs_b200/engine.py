@@ -40,6 +40,7 @@ class RunOpts(C.Structure):
                 ("refill_below", C.c_uint32), ("queue_cap", C.c_uint32), ("flags", C.c_uint32)]
 
 RUN_STAGE_TABLES = 1
+RUN_PIPELINED = 2
 
 
 # gegs_probe_state (include/gegs.h)
@@ -118,6 +119,10 @@ def check_physics(block: np.ndarray):
         raise GegsError(st, msg.value.decode())
 
 
+def _flags(stage_tables, pipelined):
+    return (RUN_STAGE_TABLES if stage_tables else 0) | (RUN_PIPELINED if pipelined else 0)
+
+
 class Engine:
     """One CUDA device + stream with the transport state (see include/gegs.h)."""
 
@@ -180,17 +185,18 @@ class Engine:
 
     def run(self, h0: int, h1: int, mode: int = MODE_PERSISTENT, batch: int = 0, blocks_per_sm: int = 0,
             threads: int = 0, max_waves: int = 0, photon_budget: int = 0, electron_budget: int = 0,
-            refill_below: int = 0, queue_cap: int = 0, stage_tables: bool = False):
+            refill_below: int = 0, queue_cap: int = 0, stage_tables: bool = False, pipelined: bool = False):
         o = RunOpts(mode, batch, blocks_per_sm, threads, max_waves, (photon_budget & 0xFFFF) | (electron_budget << 16),
-                    refill_below, queue_cap, RUN_STAGE_TABLES if stage_tables else 0)
+                    refill_below, queue_cap, _flags(stage_tables, pipelined))
         self._check(self.L.gegs_run(self.h, h0, h1, C.byref(o)))
         return self.stats()
 
     def launch(self, h0: int, h1: int, batch: int = 0, blocks_per_sm: int = 0, threads: int = 0,
-               photon_budget: int = 0, electron_budget: int = 0, refill_below: int = 0, stage_tables: bool = False):
+               photon_budget: int = 0, electron_budget: int = 0, refill_below: int = 0, stage_tables: bool = False,
+               pipelined: bool = False):
         """Queue a persistent-form run and return at once (see wait())."""
         o = RunOpts(MODE_PERSISTENT, batch, blocks_per_sm, threads, 0, (photon_budget & 0xFFFF) | (electron_budget << 16),
-                    refill_below, 0, RUN_STAGE_TABLES if stage_tables else 0)
+                    refill_below, 0, _flags(stage_tables, pipelined))
         self._check(self.L.gegs_launch(self.h, h0, h1, C.byref(o)))
 
     def wait(self):
@@ -229,7 +235,7 @@ class Engine:
     def _opts(o):
         return RunOpts(MODE_PERSISTENT, o.get("batch", 0), o.get("blocks_per_sm", 0), o.get("threads", 0), 0,
                        (o.get("photon_budget", 0) & 0xFFFF) | (o.get("electron_budget", 0) << 16),
-                       o.get("refill_below", 0), 0, RUN_STAGE_TABLES if o.get("stage_tables") else 0)
+                       o.get("refill_below", 0), 0, _flags(o.get("stage_tables"), o.get("pipelined")))
 
 
     def reset_tally(self):

@@ -71,10 +71,14 @@ typedef struct gegs_run_opts {
                                   drops the particle with a message, utility.cu:270-275) */
     uint32_t flags;            /* GEGS_RUN_STAGE_TABLES: photon consumers stage the mean-free-path and
                                   Rayleigh tables of the plan's media in shared memory (same results;
-                                  1.2 % slower on the CT 5-field plan, an autotuner choice per plan) */
+                                  1.2 % slower on the CT 5-field plan, an autotuner choice per plan);
+                                  GEGS_RUN_PIPELINED (persistent form): each wave runs the photon and
+                                  electron transports at once, then all interactions (same tally; a
+                                  particle made by an interaction is transported in the next wave) */
 } gegs_run_opts;
 
 #define GEGS_RUN_STAGE_TABLES 1u
+#define GEGS_RUN_PIPELINED 2u
 
 #define GEGS_NQUEUES 25
 

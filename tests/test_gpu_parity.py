@@ -150,6 +150,37 @@ def test_c3_full_geometry_bit_exact(engine, oracle):
     assert min(st["photon_steps_class"]) > 0 and min(st["electron_steps_class"]) > 0   # jaws, MLC, phantom
 
 
+@pytest.mark.parametrize("case", ["c3_full", "c3_small_budget1", "c2"])
+def test_pipelined_waves_bit_exact(engine, oracle, case):
+    """GEGS_RUN_PIPELINED: each wave runs the photon and electron transports at
+    once, then all eight interaction kernels; positrons that stop in the
+    electron transport annihilate in the annihilation kernel. The tally is the
+    oracle's, and the particles processed per stage and the steps taken are
+    those of the serial form (only the wave count differs)."""
+    kw = {}
+    if case == "c3_full":
+        job = W.config3(histories=30000, nphsp=30000)
+    elif case == "c3_small_budget1":
+        job = W.config3(histories=6000, nphsp=5000, dims=(48, 48, 24))
+        kw = dict(photon_budget=1, electron_budget=1)
+    else:
+        job = W.config2(histories=20000, nphsp=20000, n=40)
+    serial, ss, sh = _run(engine, job, 0, job.histories, **kw)
+    engine.reset_tally()
+    pipe = engine.run(0, job.histories, pipelined=True, **kw)
+    gpu = engine.tally()
+    ref, _ = oracle.run(job.physics, sh, 0, job.histories)
+    _assert_same(gpu, ref)
+    _assert_same(serial, ref)
+    assert pipe["error_bits"] == 0
+    assert pipe["processed"] == ss["processed"]
+    assert pipe["photon_steps"] == ss["photon_steps"] and pipe["electron_steps"] == ss["electron_steps"]
+    assert pipe["photon_steps_class"] == ss["photon_steps_class"]
+    assert pipe["electron_steps_class"] == ss["electron_steps_class"]
+    if case == "c3_full":
+        assert ss["processed"][4] > 0                      # pair production: positrons that come to rest
+
+
 def sh_dims(job):
     p = job.phantom
     return len(p["x_bounds"]) - 1, len(p["y_bounds"]) - 1, len(p["z_bounds"]) - 1
