@@ -201,8 +201,8 @@ def c5_batch(args, device):
     in one graph launch (a branch per plan), all plans launched one per stream,
     and one plan after another; then in one graph launch with options from the
     autotuner (coordinate descent over in-flight batch, grid, step budgets,
-    refill threshold and table staging, timed on a sample of each plan's
-    histories before the timed run)."""
+    refill threshold, table staging and wave order, timed on a sample of each
+    plan's histories before the timed run)."""
     from gegs_b200 import workloads as W
     from gegs_b200.batch import PlanBatch
     jobs = W.config5(n_plans=args.c5_plans, hist_min=args.c5_hist_min, hist_max=args.c5_hist_max,

@@ -40,6 +40,7 @@ TUNE_DIMENSIONS = {
     "electron_budget": lambda o: [4, 16],
     "refill_below": lambda o: [max(o["batch"] // 50, 1), max(o["batch"] // 2, 1)],
     "stage_tables": lambda o: [not o.get("stage_tables", False)],
+    "pipelined": lambda o: [not o.get("pipelined", True)],
 }
 
 
@@ -49,8 +50,9 @@ def autotune(engine, job, sample=None, candidates=None, dimensions=None, rounds=
     With `candidates`, each is timed and the fastest kept. Otherwise a
     coordinate descent: starting from choose_options, each dimension of
     TUNE_DIMENSIONS (in-flight batch, grid blocks per SM, photon and electron
-    step budgets, refill threshold, and whether the photon tables are staged
-    in shared memory, GEGS_RUN_STAGE_TABLES) tries its alternatives with the
+    step budgets, refill threshold, whether the photon tables are staged in
+    shared memory, GEGS_RUN_STAGE_TABLES, and whether a wave's two transport
+    phases run at once, GEGS_RUN_SERIAL_WAVES) tries its alternatives with the
     others fixed and keeps any that is faster; `rounds` passes over the
     dimensions.
     Every trial first runs a quarter sample untimed (graph build, queue

@@ -660,7 +660,7 @@ static gegs_status prepare_run(gegs_engine *e, uint64_t hist_begin, uint64_t his
     uint32_t max_waves = o.max_waves ? o.max_waves : 200000u;
     const uint32_t stage = (o.flags & GEGS_RUN_STAGE_TABLES) ? 1u : 0u;
     if (stage != e->ctx.stage_tables) { e->ctx.stage_tables = stage; e->ctx_gen++; }
-    const uint32_t pipe = (o.mode == GEGS_MODE_PERSISTENT && (o.flags & GEGS_RUN_PIPELINED)) ? 1u : 0u;
+    const uint32_t pipe = (o.mode == GEGS_MODE_PERSISTENT && !(o.flags & GEGS_RUN_SERIAL_WAVES)) ? 1u : 0u;
     if (pipe != e->ctx.pipelined) { e->ctx.pipelined = pipe; e->ctx_gen++; }
     uint32_t pb = (o.step_budget & 0xFFFFu) ? (o.step_budget & 0xFFFFu) : 32u;
     uint32_t eb = (o.step_budget >> 16) ? (o.step_budget >> 16) : 4u;

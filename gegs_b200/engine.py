@@ -40,7 +40,7 @@ class RunOpts(C.Structure):
                 ("refill_below", C.c_uint32), ("queue_cap", C.c_uint32), ("flags", C.c_uint32)]
 
 RUN_STAGE_TABLES = 1
-RUN_PIPELINED = 2
+RUN_SERIAL_WAVES = 2
 
 
 # gegs_probe_state (include/gegs.h)
@@ -120,7 +120,9 @@ def check_physics(block: np.ndarray):
 
 
 def _flags(stage_tables, pipelined):
-    return (RUN_STAGE_TABLES if stage_tables else 0) | (RUN_PIPELINED if pipelined else 0)
+    """gegs_run_opts.flags; `pipelined` (the default, persistent form): both
+    transport phases of a wave at once, then all interactions."""
+    return (RUN_STAGE_TABLES if stage_tables else 0) | (0 if pipelined else RUN_SERIAL_WAVES)
 
 
 class Engine:
@@ -185,7 +187,7 @@ class Engine:
 
     def run(self, h0: int, h1: int, mode: int = MODE_PERSISTENT, batch: int = 0, blocks_per_sm: int = 0,
             threads: int = 0, max_waves: int = 0, photon_budget: int = 0, electron_budget: int = 0,
-            refill_below: int = 0, queue_cap: int = 0, stage_tables: bool = False, pipelined: bool = False):
+            refill_below: int = 0, queue_cap: int = 0, stage_tables: bool = False, pipelined: bool = True):
         o = RunOpts(mode, batch, blocks_per_sm, threads, max_waves, (photon_budget & 0xFFFF) | (electron_budget << 16),
                     refill_below, queue_cap, _flags(stage_tables, pipelined))
         self._check(self.L.gegs_run(self.h, h0, h1, C.byref(o)))
@@ -193,7 +195,7 @@ class Engine:
 
     def launch(self, h0: int, h1: int, batch: int = 0, blocks_per_sm: int = 0, threads: int = 0,
                photon_budget: int = 0, electron_budget: int = 0, refill_below: int = 0, stage_tables: bool = False,
-               pipelined: bool = False):
+               pipelined: bool = True):
         """Queue a persistent-form run and return at once (see wait())."""
         o = RunOpts(MODE_PERSISTENT, batch, blocks_per_sm, threads, 0, (photon_budget & 0xFFFF) | (electron_budget << 16),
                     refill_below, 0, _flags(stage_tables, pipelined))
@@ -235,7 +237,7 @@ class Engine:
     def _opts(o):
         return RunOpts(MODE_PERSISTENT, o.get("batch", 0), o.get("blocks_per_sm", 0), o.get("threads", 0), 0,
                        (o.get("photon_budget", 0) & 0xFFFF) | (o.get("electron_budget", 0) << 16),
-                       o.get("refill_below", 0), 0, _flags(o.get("stage_tables"), o.get("pipelined")))
+                       o.get("refill_below", 0), 0, _flags(o.get("stage_tables"), o.get("pipelined", True)))
 
 
     def reset_tally(self):

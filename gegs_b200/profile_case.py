@@ -23,8 +23,9 @@ def main():
     ap.add_argument("--nphsp", type=int, default=2_000_000)
     ap.add_argument("--dims", default="256,256,120")
     ap.add_argument("--timeline", action="store_true", help="persistent form with the wave timeline")
-    ap.add_argument("--pipelined", action="store_true",
-                    help="with --timeline: both transport phases of a wave at once (GEGS_RUN_PIPELINED)")
+    ap.add_argument("--serial", action="store_true",
+                    help="with --timeline: the serial wave order (GEGS_RUN_SERIAL_WAVES) instead of both "
+                         "transport phases at once")
     ap.add_argument("--plan-histories", type=int, default=0, help="histories of the plan (fields split them; 0: --histories)")
     ap.add_argument("--first", type=int, default=0, help="first history of the run")
     ap.add_argument("--max-waves", type=int, default=0,
@@ -69,7 +70,7 @@ def main():
 
 def timeline_summary(eng, args, dims):
     import numpy as np
-    pipe = dict(pipelined=True) if getattr(args, "pipelined", False) else {}
+    pipe = dict(pipelined=False) if getattr(args, "serial", False) else {}
     eng.run(args.first, args.first + min(args.histories, 1_000_000), batch=args.batch, **pipe)   # graph and queues
     eng.set_timeline(1 << 14)
     st = eng.run(args.first, args.first + args.histories, batch=args.batch, **pipe)
@@ -104,7 +105,7 @@ def timeline_summary(eng, args, dims):
         per_phase = {k: np.round(span(g)[live], 3).tolist() for k, g in groups.items()}
     small = wave_ms < 1.0
     return {"workload": f"C3 CT head {dims[0]}x{dims[1]}x{dims[2]}, 5 fields, persistent form"
-                        + (", pipelined waves" if pipe else ""),
+                        + (", serial waves" if pipe else ", pipelined waves"),
             "histories": args.histories, "first": args.first, "batch": args.batch or "auto",
             "device_ms": st["device_ms"], "waves": st["waves"],
             "phase_ms": {k: round(v, 1) for k, v in phases.items()},

@@ -152,11 +152,11 @@ def test_c3_full_geometry_bit_exact(engine, oracle):
 
 @pytest.mark.parametrize("case", ["c3_full", "c3_small_budget1", "c2"])
 def test_pipelined_waves_bit_exact(engine, oracle, case):
-    """GEGS_RUN_PIPELINED: each wave runs the photon and electron transports at
-    once, then all eight interaction kernels; positrons that stop in the
-    electron transport annihilate in the annihilation kernel. The tally is the
-    oracle's, and the particles processed per stage and the steps taken are
-    those of the serial form (only the wave count differs)."""
+    """The persistent form's default pipelined waves (the photon and electron
+    transports at once, then all eight interaction kernels; positrons that
+    stop in the electron transport annihilate in the annihilation kernel)
+    against GEGS_RUN_SERIAL_WAVES: both tallies are the oracle's, and the
+    particles processed per stage and the steps taken are the same."""
     kw = {}
     if case == "c3_full":
         job = W.config3(histories=30000, nphsp=30000)
@@ -165,9 +165,9 @@ def test_pipelined_waves_bit_exact(engine, oracle, case):
         kw = dict(photon_budget=1, electron_budget=1)
     else:
         job = W.config2(histories=20000, nphsp=20000, n=40)
-    serial, ss, sh = _run(engine, job, 0, job.histories, **kw)
+    serial, ss, sh = _run(engine, job, 0, job.histories, pipelined=False, **kw)
     engine.reset_tally()
-    pipe = engine.run(0, job.histories, pipelined=True, **kw)
+    pipe = engine.run(0, job.histories, **kw)
     gpu = engine.tally()
     ref, _ = oracle.run(job.physics, sh, 0, job.histories)
     _assert_same(gpu, ref)
