@@ -6,13 +6,14 @@
 
 A step transports one batch of ``--hist-per-step`` histories.  ``value`` is
 the device-timed throughput (CUDA events on the engine stream) with every
-input resident in HBM; ``e2e`` repeats the steps through the C ABI from host
-memory: H2D of the step's phase-space records, the run, and D2H of the int64
-dose tally.  Multi-GPU (torchrun): each rank transports its own history range
-(weak scaling); the tallies are summed with one NCCL all-reduce.
-``--impl reference`` times the CPU restatement of the reference's routines
-(the oracle; the reference itself is CUDA-only and does not build here) on
-all host cores.
+input resident in HBM; ``e2e`` repeats the same steps through the C ABI from
+host memory: H2D of the phase-space records from pinned memory, the run, and
+D2H of the int64 dose tally into pinned memory.  Multi-GPU (torchrun): each
+rank transports its own history range (weak scaling); the tallies are summed
+with one NCCL all-reduce.
+``--impl reference`` times the reference's own stage kernels built as host
+code (``oracle/_ref``, one process per host core) on the C3 plan, or the CPU
+restatement of them (the oracle) where that build is absent.
 """
 from __future__ import annotations
 
@@ -531,7 +532,11 @@ def main():
     value = H * args.steps * world / elapsed_s
 
     # ---- end to end through the C ABI from host buffers -------------------
-    rec_per_step = int(np.ceil(H / (job.fields[0]["nrepeat"] + 1)))
+    # The same steps as the device-timed ones (same histories, same phase-space
+    # records, so the same transport work), each preceded by the upload of the
+    # whole phase space from pinned host memory and followed by the read of the
+    # tally into pinned host memory, both inside the timed region.
+    rec_per_step = len(job.phsp)
     e2e_ms = []
     try:
         import torch
@@ -545,8 +550,7 @@ def main():
     except Exception:
         host_tally = np.empty(eng.nvox, np.int64)
     for s in range(args.steps):
-        j0 = (s * rec_per_step) % max(1, len(job.phsp) - rec_per_step)
-        chunk[:] = job.phsp[j0:j0 + rec_per_step]
+        chunk[:] = job.phsp
         t = time.perf_counter()
         eng.set_phsp(chunk)
         eng.run(*hist_range(args.warmup + s), **ropt)
