@@ -180,6 +180,7 @@ struct DevCtx {
     uint32_t *trace_n;
     uint32_t trace_cap;
     const uint32_t *wave;           // wave counter (parity selects the continuation buffers)
+    const uint32_t *budget_shift;   // step budgets shifted left by this (the planner's tail setting)
     uint32_t *photon_done;          // photon MLC and phantom consumers finished in this wave
     uint32_t *electron_done;        // electron branches (jaws, MLC, phantom) finished in this wave
     uint32_t overlap;               // 1: a phase's class consumers run as concurrent graph branches

@@ -482,6 +482,7 @@ static void fill_queue_ctx(gegs_engine *e)
     Q.done = e->d_qmeta + 2 * GX_NQ;
     Q.peak = e->d_qmeta + 3 * GX_NQ;
     e->ctx.wave = &e->d_sched->waves;
+    e->ctx.budget_shift = &e->d_sched->budget_shift;
     e->ctx.photon_done = &e->d_sched->photon_done;
     e->ctx.electron_done = &e->d_sched->electron_done;
     e->ctx.overlap = 1u;
@@ -1250,6 +1251,7 @@ extern "C" gegs_status gegs_run_noalloc(gegs_engine *e, uint64_t hist_begin, uin
     c.err = err;
     c.stats = stats;
     c.wave = &sched->waves;
+    c.budget_shift = &sched->budget_shift;
     c.photon_done = &sched->photon_done;
     c.electron_done = &sched->electron_done;
     c.overlap = 0u;                 // one kernel at a time
