@@ -331,6 +331,15 @@ def sigma_series(eng, job, args, ropt, rate):
             "mean_rel_se_at_2e8": float(np.mean([x["mean_rel_se"] * np.sqrt(x["histories"] / 2e8) for x in series]))}
 
 
+def c3_config(job, hist_per_step):
+    """The workload both arms report in `config`: the C3 plan and the histories of one step."""
+    return {"workload": "C3 synthetic CT head 256x256x120 (1x1x2.5 mm), 5 coplanar fields 0/72/144/216/288 deg, "
+                        "jaws +-6 cm, 120-leaf MLC with seeded tips, 6 MV-like phase space "
+                        f"({len(job.phsp)} records, recycled)",
+            "hist_per_step": hist_per_step,
+            "l2": "working set (63 MB region table + 63 MB int64 tally + event queues) exceeds the 126 MB L2; no flush"}
+
+
 def make_job(args, histories):
     from gegs_b200 import workloads as W
     return W.config3(histories=histories, nphsp=args.nphsp)
@@ -400,10 +409,11 @@ def run_reference(args):
             "impl": "reference", "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(per_step_ms)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "C3 synthetic CT head 256x256x120, 5 fields, jaws +-6 cm, 120-leaf MLC, 6 MV-like phsp",
-                       "hist_per_step": steps_hist, "parallelism": f"{cores} host processes"},
+            "config": c3_config(job, args.hist_per_step), "parallelism": f"{cores} host processes",
+            "sample_histories_per_step": steps_hist,
             "cpu_baseline": {"value": value, "unit": "histories/s", "cores": cores, "kind": "reference",
-                             "sample": f"{steps_hist} C3 histories per step on {cores} processes: the reference's ten "
+                             "sample": f"{steps_hist} C3 histories per step (a bounded sample of the "
+                                       f"{args.hist_per_step}-history step) on {cores} processes: the reference's ten "
                                        "stage kernels and geometry compiled from its sources as host code "
                                        "(oracle/_ref, g++ -O2), draining their stacks, one process per core"},
             "e2e": {"value": value, "unit": "histories/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -424,11 +434,12 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(per_step_ms)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "C3 synthetic CT head 256x256x120, 5 fields, jaws +-6 cm, 120-leaf MLC, 6 MV-like phsp",
-                   "hist_per_step": steps_hist, "parallelism": "host threads"},
+        "config": c3_config(job, args.hist_per_step), "parallelism": f"{cores} host threads",
+        "sample_histories_per_step": steps_hist,
         "cpu_baseline": {"value": value, "unit": "histories/s", "cores": cores, "kind": "port",
-                         "sample": f"{steps_hist} C3 histories per step on {cores} threads (CPU restatement of the "
-                                   f"reference routines; the reference is CUDA-only and unbuildable here)"},
+                         "sample": f"{steps_hist} C3 histories per step (a bounded sample of the "
+                                   f"{args.hist_per_step}-history step) on {cores} threads (CPU restatement of the "
+                                   f"reference routines, used where the reference's own kernels were not built)"},
         "e2e": {"value": value, "unit": "histories/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -637,11 +648,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed_s * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "C3 synthetic CT head 256x256x120 (1x1x2.5 mm), 5 coplanar fields 0/72/144/216/288 deg, "
-                               "jaws +-6 cm, 120-leaf MLC with seeded tips, 6 MV-like phase space "
-                               f"({len(job.phsp)} records, recycled)",
-                   "hist_per_step": H, "mode": args.mode, "parallelism": f"histories sharded over {world} GPU(s)",
-                   "l2": "working set (63 MB region table + 63 MB int64 tally + event queues) exceeds the 126 MB L2; no flush"},
+        "config": c3_config(job, H), "mode": args.mode, "parallelism": f"histories sharded over {world} GPU(s)",
         "e2e": {"value": e2e, "unit": "histories/s", "h2d_bytes_per_step": rec_per_step * 28,
                 "d2h_bytes_per_step": nvox * 8},
         "roofline": {"bound": "hbm", "kernel": f"{dom_name} transport (k_{dom_name}_jaws + k_{dom_name}_mlc + k_{dom_name}, one wave)",
