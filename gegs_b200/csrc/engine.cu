@@ -517,15 +517,22 @@ static void launch_wave_kernels(gegs_engine *e, int grid, int threads)
         // pushes to a queue the other reads (a positron stopping in the
         // electron transport goes to the annihilation queue). Then all eight
         // interaction kernels, whose new particles the next wave transports.
+        // The branches are created in the order in which their blocks are best
+        // given the SMs: the jaws photons first (their long tracks keep
+        // stepping while the other branches run), then the MLC and phantom
+        // photons, then the electrons of the phantom, the MLC and the jaws.
+        // Measured on the 40M-history C3 step against the order jaws, MLC,
+        // phantom with photons and electrons interleaved: 1.7 % faster; the
+        // jaws photons created last: 6 % slower.
         fork(5);
         k_photon_jaws<<<grid, threads, ps, a[0]>>>(C);
         k_photon_mlc<<<grid, threads, ps, a[1]>>>(C);
-        k_electron_jaws<<<grid, threads, 0, a[2]>>>(C);
-        k_electron_jaws_near<<<grid, threads, 0, a[2]>>>(C);
+        k_photon<<<grid, threads, ps, s>>>(C);
+        k_electron<<<grid, threads, 0, a[4]>>>(C);
         k_electron_mlc<<<grid, threads, 0, a[3]>>>(C);
         k_electron_mlc_near<<<grid, threads, 0, a[3]>>>(C);
-        k_electron<<<grid, threads, 0, a[4]>>>(C);
-        k_photon<<<grid, threads, ps, s>>>(C);
+        k_electron_jaws<<<grid, threads, 0, a[2]>>>(C);
+        k_electron_jaws_near<<<grid, threads, 0, a[2]>>>(C);
         join(5);
         fork(7);
         k_interact<ST_COMPTON><<<grid, threads, 0, s>>>(C);
