@@ -462,6 +462,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--plan-histories", type=int, default=200_000_000,
+                    help="the C3 plan timed as one persistent launch of every field (0: skip)")
     ap.add_argument("--plain-histories", type=int, default=10_000_000,
                     help="histories of the plain-form comparison (0: skip)")
     ap.add_argument("--c4-histories", type=int, default=50_000_000,
@@ -625,6 +627,26 @@ def main():
                  "note": "both forms give the same tally bit for bit, so equal histories give equal sigma "
                          "and gamma; the ratio is the time-to-1% ratio"}
 
+    # ---- the C3 plan itself: 2e8 histories, all five fields in one launch ---
+    plan = None
+    if extras and args.plan_histories > 0:
+        pjob = make_job(args, args.plan_histories)
+        eng.set_scene(pjob.scene())
+        eng.run(0, 1_000_000, **dict(ropt, mode=MODE_PERSISTENT))     # the new scene's graph, untimed
+        pst2 = eng.run(0, pjob.histories, **dict(ropt, mode=MODE_PERSISTENT))
+        rate = pjob.histories / pst2["device_ms"] * 1e3
+        plan = {"histories": pjob.histories, "fields": len(pjob.fields), "device_s": pst2["device_ms"] / 1e3,
+                "value": rate, "waves": pst2["waves"],
+                "launch": "one persistent graph launch for every field of the plan"}
+        if plain:
+            plan["over_plain"] = rate / plain["value"]
+        if sigma:
+            n1 = sigma["time_to_1pct_s"] * value                # histories to 1 % (sigma^2 * N is constant)
+            plan["histories_to_1pct"] = n1
+            plan["time_to_1pct_s"] = n1 / rate
+            if plain:
+                plan["plain_time_to_1pct_s"] = n1 / plain["value"]
+
     # ---- C4: beamlet gradient by replay vs forward and finite differences ---
     grad = c4_gradient(args, eng) if extras and args.c4_histories > 0 else None
     nvox = eng.nvox
@@ -660,6 +682,7 @@ def main():
         "gpu_launches": int(sum(launches_per_step)),
         "clocks": clk.summary(),
         "plain_form": plain,
+        "plan_launch": plan,
         "gradient": grad,
         "batched_plans": batched,
         "stat_uncertainty": sigma,
