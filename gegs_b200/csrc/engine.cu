@@ -429,15 +429,16 @@ constexpr unsigned long long kQueueBytesPerParticle =
     cap_factor_sum() * sizeof(Part) + estate_factor_sum() * sizeof(EStatePk);
 
 // In-flight batch when the caller leaves it at 0: 60 % of the run's histories
-// in steps of 64K, between 64K and 24M (about 120 GB of queues), and within
-// 70 % of the device memory that is free once this engine's current queues are
+// in steps of 64K, between 64K and 30M (about 157 GB of queues), and within
+// 85 % of the device memory that is free once this engine's current queues are
 // counted as free. More particles in flight keep more lanes busy and need
 // fewer waves: on the CT 5-field plan's 40M-history steps, 24M in flight is
 // 2.9 % faster than 16M, 16M 7 % faster than 6M, and 26M to 30M gain nothing
-// over 24M.
+// over 24M; the whole 2e8-history plan in one launch is 1.1 % faster with 30M
+// in flight than with 25M (and 1.3 % slower with 20M).
 static uint32_t default_batch(gegs_engine *e, uint64_t histories)
 {
-    const uint64_t step = 1ull << 16, most = 24ull << 20;
+    const uint64_t step = 1ull << 16, most = 30ull << 20;
     uint64_t want = histories / 5 * 3;
     want = want / step * step;
     if (want < step) want = step;
@@ -445,7 +446,7 @@ static uint32_t default_batch(gegs_engine *e, uint64_t histories)
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
         unsigned long long have = (unsigned long long)e->batch * kQueueBytesPerParticle;
-        unsigned long long fit = (unsigned long long)((double)(free_b + have) * 0.7) / kQueueBytesPerParticle;
+        unsigned long long fit = (unsigned long long)((double)(free_b + have) * 0.85) / kQueueBytesPerParticle;
         fit = fit / step * step;
         if (want > fit) want = fit > step ? fit : step;
     }

@@ -55,8 +55,8 @@ typedef enum gegs_mode {
 typedef struct gegs_run_opts {
     int32_t mode;              /* gegs_mode */
     uint32_t batch;            /* particles kept in flight (0 = 60 % of the run's histories in steps of 64K,
-                                  64K to 24M, within 70 % of free device memory; queue memory ~5 KB each,
-                                  ~120 GB at 24M) */
+                                  64K to 30M, within 85 % of free device memory; queue memory ~5 KB each,
+                                  ~157 GB at 30M) */
     int32_t blocks_per_sm;     /* 0 = default (6: grid = 6 x SM count) */
     int32_t threads_per_block; /* 0 = default */
     uint32_t max_waves;        /* safety budget (0 = default) */
