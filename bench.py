@@ -4,7 +4,10 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gegs|reference]
 
-A step transports one batch of ``--hist-per-step`` histories.  ``value`` is
+A step transports the whole C3 plan, ``--hist-per-step`` histories (2e8) over
+all five fields, in one persistent launch; each step takes its own histories
+(the plan's field ranges moved along the history index), so no step repeats
+another's random numbers.  ``value`` is
 the device-timed throughput (CUDA events on the engine stream) with every
 input resident in HBM; ``e2e`` repeats the same steps through the C ABI from
 host memory: H2D of the phase-space records from pinned memory, the run, and
@@ -451,7 +454,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gegs", choices=["gegs", "reference"])
-    ap.add_argument("--hist-per-step", type=int, default=40_000_000)
+    ap.add_argument("--hist-per-step", type=int, default=200_000_000,
+                    help="histories of the plan that one step transports, over all five fields in one launch")
     ap.add_argument("--nphsp", type=int, default=10_000_000)
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--mode", default="persistent", choices=["persistent", "plain", "timed"],
@@ -462,8 +466,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--plan-histories", type=int, default=200_000_000,
-                    help="the C3 plan timed as one persistent launch of every field (0: skip)")
+    ap.add_argument("--roofline-histories", type=int, default=10_000_000,
+                    help="histories of the timed-form run that times each transport kernel for the roofline")
     ap.add_argument("--plain-histories", type=int, default=10_000_000,
                     help="histories of the plain-form comparison (0: skip)")
     ap.add_argument("--c4-histories", type=int, default=50_000_000,
@@ -500,8 +504,7 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     H = args.hist_per_step
-    total = H * (args.warmup + args.steps) * world
-    job = make_job(args, max(total, 200_000_000))
+    job = make_job(args, H)                       # the plan: five fields of H/5 histories
     sh = job.scene()
     mode = {"persistent": MODE_PERSISTENT, "plain": MODE_PLAIN, "timed": MODE_TIMED}[args.mode]
     ropt = dict(mode=mode, batch=args.batch, photon_budget=args.photon_budget, electron_budget=args.electron_budget)
@@ -510,7 +513,11 @@ def main():
     eng.set_scene(sh)
 
     def hist_range(step):
+        """Histories [base, base + H) of a step, with the plan's fields moved
+        there (gegs_set_field: history ranges only; the phantom stays)."""
         base = (rank * (args.warmup + args.steps) + step) * H
+        for i, f in enumerate(job.fields):
+            eng.set_field(i, dict(f, hist_begin=f["hist_begin"] + base, hist_end=f["hist_end"] + base))
         return base, base + H
 
     for s in range(args.warmup):
@@ -526,7 +533,8 @@ def main():
     with ClockSampler(local) as clk:
         t0 = time.perf_counter()
         for s in range(args.warmup, args.warmup + args.steps):
-            st = eng.run(*hist_range(s), **ropt)
+            h0, h1 = hist_range(s)
+            st = eng.run(h0, h1, **ropt)
             dev_ms.append(st["device_ms"])
             stats.append(st)
         if dist is not None:
@@ -566,7 +574,8 @@ def main():
         chunk[:] = job.phsp
         t = time.perf_counter()
         eng.set_phsp(chunk)
-        eng.run(*hist_range(args.warmup + s), **ropt)
+        h0, h1 = hist_range(args.warmup + s)
+        eng.run(h0, h1, **ropt)
         eng.tally(out=host_tally)
         e2e_ms.append((time.perf_counter() - t) * 1e3)
     e2e = H * args.steps * world / (sum(e2e_ms) / 1e3)
@@ -588,7 +597,10 @@ def main():
 
     # ---- roofline of the dominant kernel (timed mode, outside the timed region)
     eng.set_phsp(job.phsp)
-    tst = eng.run(0, H // 4, **dict(ropt, mode=MODE_TIMED))
+    for i, f in enumerate(job.fields):                  # the plan's own history ranges again
+        eng.set_field(i, f)
+    RH = args.roofline_histories                       # the timed form over the first histories of the plan
+    tst = eng.run(0, RH, **dict(ropt, mode=MODE_TIMED))
     kinds = ["photon", "compton", "photo", "rayleigh", "pair", "electron", "moller", "brems", "bhabha", "annih",
              "source", "planner", "photon_jaws", "electron_jaws", "photon_mlc", "electron_mlc"]
     ms = np.array(tst["stage_ms"][:16])
@@ -601,7 +613,7 @@ def main():
     dom = kinds.index(dom_name)
     launches = max(1, tst["stage_launches"][dom])              # waves that ran this stage
     per_stage_bytes, ost = algorithmic_bytes(job, sample=20000)
-    alg_bytes_per_launch = per_stage_bytes[dom] * (H // 4) / launches
+    alg_bytes_per_launch = per_stage_bytes[dom] * RH / launches
     avg_launch_s = stage_ms[dom_name] / 1e3 / launches
     peak, peak_kind = hbm_peak()
     achieved = alg_bytes_per_launch / avg_launch_s / 1e9
@@ -624,28 +636,14 @@ def main():
                                             "counter read-back after every kernel (CUDA_EGS.cu:226-365, 498-799)",
                  "value": hp / pst["device_ms"] * 1e3, "persistent_value": hp / qst["device_ms"] * 1e3,
                  "persistent_over_plain": pst["device_ms"] / qst["device_ms"],
+                 "plan_over_plain": value / (hp / pst["device_ms"] * 1e3),
                  "note": "both forms give the same tally bit for bit, so equal histories give equal sigma "
-                         "and gamma; the ratio is the time-to-1% ratio"}
-
-    # ---- the C3 plan itself: 2e8 histories, all five fields in one launch ---
-    plan = None
-    if extras and args.plan_histories > 0:
-        pjob = make_job(args, args.plan_histories)
-        eng.set_scene(pjob.scene())
-        eng.run(0, 1_000_000, **dict(ropt, mode=MODE_PERSISTENT))     # the new scene's graph, untimed
-        pst2 = eng.run(0, pjob.histories, **dict(ropt, mode=MODE_PERSISTENT))
-        rate = pjob.histories / pst2["device_ms"] * 1e3
-        plan = {"histories": pjob.histories, "fields": len(pjob.fields), "device_s": pst2["device_ms"] / 1e3,
-                "value": rate, "waves": pst2["waves"],
-                "launch": "one persistent graph launch for every field of the plan"}
-        if plain:
-            plan["over_plain"] = rate / plain["value"]
+                         "and gamma; a ratio of rates is the time-to-1% ratio. persistent_over_plain: the same "
+                         "10M histories; plan_over_plain: the bench's steps (the whole plan per launch)"}
         if sigma:
-            n1 = sigma["time_to_1pct_s"] * value                # histories to 1 % (sigma^2 * N is constant)
-            plan["histories_to_1pct"] = n1
-            plan["time_to_1pct_s"] = n1 / rate
-            if plain:
-                plan["plain_time_to_1pct_s"] = n1 / plain["value"]
+            n1 = sigma["time_to_1pct_s"] * value            # histories to 1 % (sigma^2 N is constant)
+            plain["histories_to_1pct"] = n1
+            plain["time_to_1pct_s"] = n1 / plain["value"]
 
     # ---- C4: beamlet gradient by replay vs forward and finite differences ---
     grad = c4_gradient(args, eng) if extras and args.c4_histories > 0 else None
@@ -682,7 +680,6 @@ def main():
         "gpu_launches": int(sum(launches_per_step)),
         "clocks": clk.summary(),
         "plain_form": plain,
-        "plan_launch": plan,
         "gradient": grad,
         "batched_plans": batched,
         "stat_uncertainty": sigma,
